@@ -1,0 +1,374 @@
+// C ABI entry points (include/gb200.h).  Every call catches gb200::Error and
+// other exceptions and turns them into status codes plus a message kept in
+// the context (gb200_last_error); nothing throws across the C boundary.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "context.cuh"
+#include "split.cuh"
+
+using namespace gb200;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+template <typename F>
+int guarded(gb200_context* ctx, F&& f) {
+  Context* c = reinterpret_cast<Context*>(ctx);
+  try {
+    if (!c) throw Error(GB200_ERR_INVALID, "null context");
+    GB_CUDA(cudaSetDevice(c->device));
+    f(*c);
+    c->last_error.clear();
+    return GB200_OK;
+  } catch (const Error& e) {
+    if (c) c->last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    if (c) c->last_error = "host allocation failed";
+    return GB200_ERR_OOM;
+  } catch (const std::exception& e) {
+    if (c) c->last_error = e.what();
+    return GB200_ERR_INVALID;
+  }
+}
+
+// Scatter a chunk of stored pairs (k1 >= k2, index k1(k1+1)/2 + k2) into the
+// full [nk][nk] storage: (k1,k2) directly and, for k1 > k2, (k2,k1) as the
+// per-Q conjugate transpose (df_integral_t.h:68,169-176).
+__global__ void scatter_pairs_kernel(const cplx* half_chunk, int64_t p0, int64_t cnt, cplx* full, int nk, int NQ,
+                                     int nao) {
+  const int64_t m2 = (int64_t)nao * nao;
+  const int64_t pe = (int64_t)NQ * m2;
+  const int64_t total = cnt * pe;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lp = e / pe;
+    int64_t r = e - lp * pe;
+    int64_t idx = p0 + lp;
+    int64_t k1 = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+    while (k1 * (k1 + 1) / 2 > idx) --k1;
+    while ((k1 + 1) * (k1 + 2) / 2 <= idx) ++k1;
+    int64_t k2 = idx - k1 * (k1 + 1) / 2;
+    int64_t Q = r / m2;
+    int ij = (int)(r - Q * m2);
+    int i = ij / nao, j = ij % nao;
+    cplx v = half_chunk[e];
+    full[(k1 * nk + k2) * pe + r] = v;
+    if (k1 != k2) full[(k2 * nk + k1) * pe + Q * m2 + (int64_t)j * nao + i] = cconj(v);
+  }
+}
+
+void upload_integrals(Context& c, DevArray<cplx>& dst, const double* V_half, int64_t npairs) {
+  const int nk = c.d.nk;
+  const int64_t pe = c.pair_elems();
+  require(npairs == (int64_t)nk * (nk + 1) / 2, GB200_ERR_INVALID, "set_integrals: npairs must be nk(nk+1)/2");
+  dst.alloc((size_t)nk * nk * pe);
+  // stream the half storage through a bounded staging buffer
+  const int64_t chunk_pairs = std::max<int64_t>(1, std::min<int64_t>(npairs, (int64_t)(1e9 / (pe * sizeof(cplx)))));
+  DevArray<cplx> stage;
+  stage.alloc((size_t)chunk_pairs * pe);
+  for (int64_t p0 = 0; p0 < npairs; p0 += chunk_pairs) {
+    int64_t cnt = std::min(chunk_pairs, npairs - p0);
+    GB_CUDA(cudaMemcpyAsync(stage.p, reinterpret_cast<const cplx*>(V_half) + p0 * pe,
+                            (size_t)cnt * pe * sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
+    scatter_pairs_kernel<<<148 * 16, 256, 0, c.stream>>>(stage.p, p0, cnt, dst.p, nk, c.d.NQ, c.d.nao);
+    GB_CHECK_LAUNCH();
+    GB_CUDA(cudaStreamSynchronize(c.stream));
+  }
+}
+
+struct HostIO {
+  // pinned-free staging: plain cudaMemcpy from pageable host memory
+  static void h2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    GB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+  }
+  static void d2h(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    GB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+const char* gb200_version(void) { return "gb200 0.1.0 (integral format 1.0.0)"; }
+
+// CheckVersion (common_defs.h:191-212): accept v >= 1.0.0 on major.minor.patch.
+int gb200_check_integral_version(const char* v) {
+  if (!v) return GB200_ERR_INVALID;
+  int a = 0, b = 0, p = 0;
+  char suffix[32] = "";
+  int parsed = std::sscanf(v, "%d.%d.%d%31s", &a, &b, &p, suffix);
+  if (parsed < 3) return GB200_ERR_INVALID;
+  const int ref[3] = {1, 0, 0};
+  bool ok;
+  if (a != ref[0]) ok = a > ref[0];
+  else if (b != ref[1]) ok = b > ref[1];
+  else if (p != ref[2]) ok = p > ref[2];
+  else ok = true;
+  return ok ? GB200_OK : GB200_ERR_OUTDATED_INPUT;
+}
+
+int gb200_create(const gb200_dims* dims, int device, gb200_context** out) {
+  if (!dims || !out) return GB200_ERR_INVALID;
+  *out = nullptr;
+  const gb200_dims& d = *dims;
+  if (d.nk <= 0 || d.nao <= 0 || d.NQ <= 0 || d.nts <= 0 || d.nw <= 0 || d.nw_b <= 0 || !(d.beta > 0)) {
+    g_create_error = "gb200_create: non-positive dimension";
+    return GB200_ERR_INVALID;
+  }
+  if (d.ns != 1 && d.ns != 2) { g_create_error = "gb200_create: ns must be 1 or 2"; return GB200_ERR_INVALID; }
+  if (d.nso != d.nao) { g_create_error = "gb200_create: two-component (X2C) input is not supported"; return GB200_ERR_INVALID; }
+  if (d.nso > 64) { g_create_error = "gb200_create: nso > 64 is not supported"; return GB200_ERR_INVALID; }
+  if (d.nts % 2 != 0) { g_create_error = "Number of tau points should be even!!!"; return GB200_ERR_WRONG_GRID; }
+  Context* c = nullptr;
+  try {
+    int ndev = 0;
+    GB_CUDA(cudaGetDeviceCount(&ndev));
+    require(device >= 0 && device < ndev, GB200_ERR_INVALID, "gb200_create: bad device index");
+    GB_CUDA(cudaSetDevice(device));
+    c = new Context();
+    c->d = d;
+    c->device = device;
+    GB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  } catch (const Error& e) {
+    g_create_error = e.what();
+    delete c;
+    return e.code;
+  }
+  *out = reinterpret_cast<gb200_context*>(c);
+  return GB200_OK;
+}
+
+void gb200_destroy(gb200_context* ctx) {
+  Context* c = reinterpret_cast<Context*>(ctx);
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  split_release(*c);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char* gb200_last_error(const gb200_context* ctx) {
+  const Context* c = reinterpret_cast<const Context*>(ctx);
+  return c ? c->last_error.c_str() : g_create_error.c_str();
+}
+
+int gb200_set_kq_maps(gb200_context* ctx, const int32_t* kplus, const int32_t* kminus) {
+  return guarded(ctx, [&](Context& c) {
+    require(kplus && kminus, GB200_ERR_INVALID, "set_kq_maps: null pointer");
+    const int nk = c.d.nk;
+    c.kplus.assign(kplus, kplus + (size_t)nk * nk);
+    c.kminus.assign(kminus, kminus + (size_t)nk * nk);
+    for (size_t i = 0; i < c.kplus.size(); ++i)
+      require(c.kplus[i] >= 0 && c.kplus[i] < nk && c.kminus[i] >= 0 && c.kminus[i] < nk, GB200_ERR_INVALID,
+              "set_kq_maps: k index out of range");
+    build_tables(c);
+    c.have_kq = true;
+  });
+}
+
+int gb200_set_grid(gb200_context* ctx, const double* Tnt_f, const double* Ttn_f, const double* Tnt_b,
+                   const double* Ttn_b, const double* wsample_f) {
+  return guarded(ctx, [&](Context& c) {
+    require(Tnt_f && Ttn_f && Tnt_b && Ttn_b && wsample_f, GB200_ERR_INVALID, "set_grid: null pointer");
+    const gb200_dims& d = c.d;
+    c.Tnt_f.upload(reinterpret_cast<const cplx*>(Tnt_f), (size_t)d.nw * d.nts, c.stream);
+    c.Ttn_f.upload(reinterpret_cast<const cplx*>(Ttn_f), (size_t)d.nts * d.nw, c.stream);
+    c.Tnt_b.upload(reinterpret_cast<const cplx*>(Tnt_b), (size_t)d.nw_b * d.nts, c.stream);
+    c.Ttn_b.upload(reinterpret_cast<const cplx*>(Ttn_b), (size_t)d.nts * d.nw_b, c.stream);
+    c.wsample_f.assign(wsample_f, wsample_f + d.nw);
+    const cplx* tb = reinterpret_cast<const cplx*>(Ttn_f) + (size_t)(d.nts - 1) * d.nw;
+    c.Ttn_beta.assign(tb, tb + d.nw);
+    GB_CUDA(cudaStreamSynchronize(c.stream));
+    c.have_grid = true;
+  });
+}
+
+int gb200_set_integrals(gb200_context* ctx, int which, const double* V_half, int64_t npairs) {
+  return guarded(ctx, [&](Context& c) {
+    require(V_half != nullptr, GB200_ERR_INVALID, "set_integrals: null pointer");
+    if (which == GB200_INTEGRALS_GW) {
+      upload_integrals(c, c.V, V_half, npairs);
+      c.have_V = true;
+      split_invalidate(c);
+    } else if (which == GB200_INTEGRALS_HF) {
+      upload_integrals(c, c.Vhf, V_half, npairs);
+      c.have_Vhf = true;
+    } else {
+      throw Error(GB200_ERR_INVALID, "set_integrals: unknown integral set");
+    }
+  });
+}
+
+int gb200_set_precision(gb200_context* ctx, int mode, int slices) {
+  return guarded(ctx, [&](Context& c) {
+    require(mode == GB200_PREC_FP64 || mode == GB200_PREC_SPLIT, GB200_ERR_INVALID, "set_precision: unknown mode");
+    if (mode == GB200_PREC_SPLIT)
+      require(slices >= 2 && slices <= 8, GB200_ERR_INVALID, "set_precision: slices must be in [2, 8]");
+    if (mode != c.prec_mode || slices != c.slices) split_invalidate(c);
+    c.prec_mode = mode;
+    c.slices = slices;
+  });
+}
+
+int gb200_gw_sigma(gb200_context* ctx, const double* G, double* Sigma) {
+  return guarded(ctx, [&](Context& c) {
+    require(G && Sigma, GB200_ERR_INVALID, "gw_sigma: null pointer");
+    const size_t bytes = c.g_elems() * sizeof(cplx);
+    cplx* dG = (cplx*)c.scratch.get(SL_IO_G, bytes);
+    cplx* dS = (cplx*)c.scratch.get(SL_IO_S, bytes);
+    HostIO::h2d(dG, G, bytes, c.stream);
+    gw_sigma(c, dG, dS, c.stream);
+    HostIO::d2h(Sigma, dS, bytes, c.stream);
+    GB_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int gb200_gw_sigma_device(gb200_context* ctx, const double* G_dev, double* Sigma_dev, void* stream) {
+  return guarded(ctx, [&](Context& c) {
+    require(G_dev && Sigma_dev, GB200_ERR_INVALID, "gw_sigma_device: null pointer");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+    gw_sigma(c, reinterpret_cast<const cplx*>(G_dev), reinterpret_cast<cplx*>(Sigma_dev), st);
+  });
+}
+
+int gb200_hf_fock(gb200_context* ctx, const double* dm, const double* S, double madelung, double* F) {
+  return guarded(ctx, [&](Context& c) {
+    require(dm && S && F, GB200_ERR_INVALID, "hf_fock: null pointer");
+    const size_t bytes = c.mat_elems() * sizeof(cplx);
+    cplx* ddm = (cplx*)c.scratch.get(SL_DM, bytes);
+    cplx* dS = (cplx*)c.scratch.get(SL_IO_H, bytes);
+    cplx* dF = (cplx*)c.scratch.get(SL_IO_S1, bytes);
+    HostIO::h2d(ddm, dm, bytes, c.stream);
+    HostIO::h2d(dS, S, bytes, c.stream);
+    hf_fock(c, ddm, dS, madelung, dF, c.stream);
+    HostIO::d2h(F, dF, bytes, c.stream);
+    GB_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int gb200_hf_fock_device(gb200_context* ctx, const double* dm_dev, const double* S_dev, double madelung,
+                         double* F_dev, void* stream) {
+  return guarded(ctx, [&](Context& c) {
+    require(dm_dev && S_dev && F_dev, GB200_ERR_INVALID, "hf_fock_device: null pointer");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+    hf_fock(c, reinterpret_cast<const cplx*>(dm_dev), reinterpret_cast<const cplx*>(S_dev), madelung,
+            reinterpret_cast<cplx*>(F_dev), st);
+  });
+}
+
+int gb200_dyson_set_hamiltonian(gb200_context* ctx, const double* H, const double* S) {
+  return guarded(ctx, [&](Context& c) {
+    require(H && S, GB200_ERR_INVALID, "dyson_set_hamiltonian: null pointer");
+    c.H.upload(reinterpret_cast<const cplx*>(H), c.mat_elems(), c.stream);
+    c.S.upload(reinterpret_cast<const cplx*>(S), c.mat_elems(), c.stream);
+    // dyson.cpp:44-45: S_k and H_k are hermitized on input
+    hermitize_batched(c.H.get(), (int64_t)c.d.ns * c.d.nk, c.d.nso, 1.0, c.stream);
+    hermitize_batched(c.S.get(), (int64_t)c.d.ns * c.d.nk, c.d.nso, 1.0, c.stream);
+    GB_CUDA(cudaStreamSynchronize(c.stream));
+    c.have_H = true;
+  });
+}
+
+static void upload_sigmas(Context& c, const double* Sigma1, const double* Sigma_tau, cplx** d1, cplx** dt) {
+  const size_t b1 = c.mat_elems() * sizeof(cplx), bt = c.g_elems() * sizeof(cplx);
+  *d1 = (cplx*)c.scratch.get(SL_IO_S1, b1);
+  *dt = (cplx*)c.scratch.get(SL_IO_S, bt);
+  HostIO::h2d(*d1, Sigma1, b1, c.stream);
+  HostIO::h2d(*dt, Sigma_tau, bt, c.stream);
+}
+
+int gb200_dyson_find_mu(gb200_context* ctx, const double* Sigma1, const double* Sigma_tau, double mu0,
+                        double nel_target, double tol, double* mu_out, double* nel_out) {
+  return guarded(ctx, [&](Context& c) {
+    require(Sigma1 && Sigma_tau && mu_out, GB200_ERR_INVALID, "find_mu: null pointer");
+    require(nel_target > 0 && tol > 0, GB200_ERR_INVALID, "find_mu: nel and tol must be positive");
+    cplx *d1, *dt;
+    upload_sigmas(c, Sigma1, Sigma_tau, &d1, &dt);
+    // selfenergy_eigenspectra (dyson.cpp:48-70) reads the self-energies as given
+    dyson_prepare_X(c, d1, dt, false, c.stream);
+    *mu_out = dyson_find_mu(c, mu0, nel_target, tol, nel_out, c.stream);
+  });
+}
+
+int gb200_dyson_electrons(gb200_context* ctx, const double* Sigma1, const double* Sigma_tau, double mu,
+                          double* nel_out) {
+  return guarded(ctx, [&](Context& c) {
+    require(Sigma1 && Sigma_tau && nel_out, GB200_ERR_INVALID, "dyson_electrons: null pointer");
+    cplx *d1, *dt;
+    upload_sigmas(c, Sigma1, Sigma_tau, &d1, &dt);
+    dyson_prepare_X(c, d1, dt, false, c.stream);
+    *nel_out = dyson_electrons_prepared(c, mu, c.stream);
+  });
+}
+
+int gb200_dyson_compute_G(gb200_context* ctx, double* Sigma1, double* Sigma_tau, double mu, double* G) {
+  return guarded(ctx, [&](Context& c) {
+    require(Sigma1 && Sigma_tau && G, GB200_ERR_INVALID, "compute_G: null pointer");
+    cplx *d1, *dt;
+    upload_sigmas(c, Sigma1, Sigma_tau, &d1, &dt);
+    cplx* dG = (cplx*)c.scratch.get(SL_IO_G, c.g_elems() * sizeof(cplx));
+    dyson_compute_G(c, d1, dt, mu, dG, c.stream);
+    HostIO::d2h(Sigma1, d1, c.mat_elems() * sizeof(cplx), c.stream);
+    HostIO::d2h(Sigma_tau, dt, c.g_elems() * sizeof(cplx), c.stream);
+    HostIO::d2h(G, dG, c.g_elems() * sizeof(cplx), c.stream);
+    GB_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int gb200_energy(gb200_context* ctx, const double* G, const double* Sigma1, const double* Sigma_tau, double* e3) {
+  return guarded(ctx, [&](Context& c) {
+    require(G && Sigma1 && Sigma_tau && e3, GB200_ERR_INVALID, "energy: null pointer");
+    cplx *d1, *dt;
+    upload_sigmas(c, Sigma1, Sigma_tau, &d1, &dt);
+    cplx* dG = (cplx*)c.scratch.get(SL_IO_G, c.g_elems() * sizeof(cplx));
+    HostIO::h2d(dG, G, c.g_elems() * sizeof(cplx), c.stream);
+    energy(c, dG, d1, dt, e3, c.stream);
+  });
+}
+
+int gb200_iteration_device(gb200_context* ctx, double* G_dev, double* Sigma1_dev, double* Sigma_dev,
+                           double madelung, double nel_target, double tol, double* mu_inout, double* e_out3,
+                           void* stream) {
+  return guarded(ctx, [&](Context& c) {
+    require(G_dev && Sigma1_dev && Sigma_dev && mu_inout, GB200_ERR_INVALID, "iteration: null pointer");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+    const gb200_dims& d = c.d;
+    cplx* G = reinterpret_cast<cplx*>(G_dev);
+    cplx* S1 = reinterpret_cast<cplx*>(Sigma1_dev);
+    cplx* St = reinterpret_cast<cplx*>(Sigma_dev);
+    const int64_t me = c.mat_elems();
+    // dm = spin_prefactor * G(beta) (hf_solver.cpp:9-16)
+    cplx* dm = (cplx*)c.scratch.get(SL_DM, me * sizeof(cplx));
+    GB_CUDA(cudaMemcpyAsync(dm, G + (int64_t)(d.nts - 1) * me, me * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
+    scale_inplace(dm, me, d.ns == 2 ? -1.0 : -2.0, st);
+    require(c.have_H, GB200_ERR_STATE, "iteration: Hamiltonian/overlap must be set");
+    hf_fock(c, dm, c.S.get(), madelung, S1, st);
+    gw_sigma(c, G, St, st);
+    double mu = *mu_inout;
+    if (nel_target > 0) {
+      dyson_prepare_X(c, S1, St, false, st);
+      mu = dyson_find_mu(c, mu, nel_target, tol, nullptr, st);
+    }
+    dyson_compute_G(c, S1, St, mu, G, st);
+    *mu_inout = mu;
+    if (e_out3) energy(c, G, S1, St, e_out3, st);
+    GB_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int gb200_last_timings(const gb200_context* ctx, float* out4) {
+  const Context* c = reinterpret_cast<const Context*>(ctx);
+  if (!c || !out4) return GB200_ERR_INVALID;
+  std::memcpy(out4, c->timings, sizeof(c->timings));
+  return GB200_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,113 @@
+// The context behind the C ABI: dimensions, resident device inputs, the
+// scratch arena and the per-q offset tables of the k +- q maps.
+#pragma once
+
+#include <cstdio>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace gb200 {
+
+// Owning device allocation.
+template <typename T>
+struct DevArray {
+  T* p = nullptr;
+  size_t n = 0;
+  DevArray() = default;
+  DevArray(const DevArray&) = delete;
+  DevArray& operator=(const DevArray&) = delete;
+  ~DevArray() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count <= n && p) return;
+    release();
+    if (count == 0) return;
+    GB_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void upload(const T* host, size_t count, cudaStream_t st) {
+    alloc(count);
+    GB_CUDA(cudaMemcpyAsync(p, host, count * sizeof(T), cudaMemcpyHostToDevice, st));
+  }
+  T* get() const { return p; }
+};
+
+// Named scratch buffers that only grow.
+struct Scratch {
+  std::vector<std::unique_ptr<DevArray<char>>> bufs;
+  void* get(int slot, size_t bytes) {
+    if ((int)bufs.size() <= slot) bufs.resize(slot + 1);
+    if (!bufs[slot]) bufs[slot].reset(new DevArray<char>());
+    bufs[slot]->alloc(bytes);
+    return bufs[slot]->p;
+  }
+  void release() { bufs.clear(); }
+};
+
+enum ScratchSlot {
+  SL_T1 = 0, SL_BT, SL_P0, SL_PW, SL_AUG, SL_TMP, SL_Y1, SL_Y2,
+  SL_HF_Y, SL_HF_U, SL_HF_DMT, SL_DY_SW, SL_DY_GW, SL_DY_X, SL_RED, SL_IO_G, SL_IO_S,
+  SL_IO_S1, SL_IO_H, SL_DM, SL_PINV, SL_SPLIT0, SL_COUNT
+};
+
+struct Context {
+  gb200_dims d{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  int prec_mode = GB200_PREC_FP64;
+  int slices = 4;
+
+  bool have_kq = false, have_grid = false, have_V = false, have_Vhf = false, have_H = false;
+  std::vector<int32_t> kplus, kminus;  // [nk * nk]
+
+  // transforms
+  DevArray<cplx> Tnt_f, Ttn_f, Tnt_b, Ttn_b;
+  std::vector<double> wsample_f;
+  std::vector<cplx> Ttn_beta;  // host copy of the tau = beta row of Ttn_f
+
+  // integrals, all ordered pairs [nk][nk][NQ][nao][nao]
+  DevArray<cplx> V, Vhf;
+  // Dyson inputs [ns][nk][nso][nso]
+  DevArray<cplx> H, S;
+
+  // per-q offset tables (device): [nq][nk] or [nq][nk*ns]
+  DevArray<int64_t> tab_pair_plus, tab_pair_minus, tab_g_plus, tab_g_minus, tab_pair_plus_ns;
+  DevArray<int64_t> tab_pair_diag_ns;  // HF: pair (k,k) offset for index k*ns+s
+
+  Scratch scratch;
+  float timings[4] = {0, 0, 0, 0};
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+
+  int64_t nao() const { return d.nao; }
+  int64_t pair_elems() const { return (int64_t)d.NQ * d.nao * d.nao; }
+  int64_t g_elems() const { return (int64_t)d.nts * d.ns * d.nk * d.nso * d.nso; }
+  int64_t mat_elems() const { return (int64_t)d.ns * d.nk * d.nso * d.nso; }
+};
+
+// stages implemented in the .cu files
+void build_tables(Context& c);
+void build_hf_tables(Context& c);
+void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st);
+void hf_fock(Context& c, const cplx* dm, const cplx* S, double madelung, cplx* F, cudaStream_t st);
+void dyson_compute_G(Context& c, cplx* Sigma1, cplx* Sigma_tau, double mu, cplx* G, cudaStream_t st);
+void dyson_prepare_X(Context& c, cplx* Sigma1, cplx* Sigma_tau, bool hermitize, cudaStream_t st);
+double dyson_electrons_prepared(Context& c, double mu, cudaStream_t st);
+double dyson_find_mu(Context& c, double mu0, double nel_target, double tol, double* nel_out, cudaStream_t st);
+void energy(Context& c, const cplx* G, const cplx* Sigma1, const cplx* Sigma_tau, double* e3, cudaStream_t st);
+
+// linear algebra helpers (linalg.cu)
+void hermitize_batched(cplx* X, int64_t nmat, int n, double scale, cudaStream_t st);
+void invert_small_batched(const cplx* A, cplx* Ainv, int64_t nmat, int n, cudaStream_t st);
+void invert_large_batched(const cplx* A, cplx* Ainv, cplx* aug, int64_t nmat, int n, bool herm_from_lower,
+                          bool identity_minus, cudaStream_t st);
+void scale_inplace(cplx* X, int64_t count, double s, cudaStream_t st);
+
+}  // namespace gb200

@@ -1,0 +1,268 @@
+// GW self-energy on one GPU: P0(tau,q) -> W(tau,q) -> Sigma(tau,k).
+//
+// Follows gw_cpu_kernel::solve (green-mbpt src/gw_cpu_kernel.cpp:31-134) with
+// the MPI decomposition replaced by batched device contractions:
+//  * the q loop stays (the reference's internode loop, :45-48);
+//  * the k1 and tau loops become batch dimensions of one GEMM per step,
+//    blocked over k to bound the intermediates;
+//  * the three ZGEMMs per (q,k,tau) of P0_contraction (:200-215) and
+//    selfenergy_contraction (:359-373) become three batched GEMMs each:
+//      P0:    T1 = V G(tau,k+q);  Bt = Gbar(beta-tau,k) T1;  P0 -= pref Bt . conj(V)
+//      Sigma: Y1 = V G(tau,k-q);  Y2 = Y1^T W(tau);           Sigma -= Y2 . conj(V)
+//    which is the same sum, P0_QQ' = -pref sum Gbar_tp V^Q_pm G_mn conj(V^Q'_tn),
+//    Sigma_ij = -sum V^Q_im G_mn W_QQ' conj(V^Q'_jn), in a batched order.
+#include <algorithm>
+
+#include "context.cuh"
+#include "split.cuh"
+
+namespace gb200 {
+namespace {
+
+// P0(t) = herm(P0(t)/nk), P0(nts-1-t) = P0(t) for t < nts/2 (gw_cpu_kernel.cpp:217-225).
+__global__ void symmetrize_p0_kernel(cplx* P0, int nts, int NQ, double inv_nk) {
+  const int nth = nts / 2;
+  const int64_t npairs = (int64_t)NQ * (NQ + 1) / 2;
+  const int64_t total = (int64_t)nth * npairs;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    int t = (int)(e / npairs);
+    int64_t p = e - (int64_t)t * npairs;
+    int i = (int)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
+    while ((int64_t)i * (i + 1) / 2 > p) --i;
+    while ((int64_t)(i + 1) * (i + 2) / 2 <= p) ++i;
+    int j = (int)(p - (int64_t)i * (i + 1) / 2);
+    cplx* M = P0 + (int64_t)t * NQ * NQ;
+    cplx* Mm = P0 + (int64_t)(nts - 1 - t) * NQ * NQ;
+    cplx a = cscale(M[(int64_t)i * NQ + j], inv_nk);
+    cplx b = cscale(M[(int64_t)j * NQ + i], inv_nk);
+    cplx h = cscale(cadd(a, cconj(b)), 0.5);
+    M[(int64_t)i * NQ + j] = h;
+    M[(int64_t)j * NQ + i] = cconj(h);
+    Mm[(int64_t)i * NQ + j] = h;
+    Mm[(int64_t)j * NQ + i] = cconj(h);
+  }
+}
+
+inline unsigned grid_for(int64_t n, int nt) {
+  int64_t g = (n + nt - 1) / nt;
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
+}
+
+// Dense row-major matrix view helper.
+ZOperand dense(const cplx* p, int64_t ld) {
+  ZOperand o;
+  o.ptr = p;
+  o.row = lin(ld);
+  o.col = lin(1);
+  return o;
+}
+
+}  // namespace
+
+void build_tables(Context& c) {
+  const int nk = c.d.nk, ns = c.d.ns;
+  const int64_t pe = c.pair_elems();
+  const int64_t ge = (int64_t)c.d.nso * c.d.nso;
+  std::vector<int64_t> pp(nk * nk), pm(nk * nk), gp(nk * nk), gm(nk * nk), ppns((size_t)nk * nk * ns);
+  for (int q = 0; q < nk; ++q)
+    for (int k = 0; k < nk; ++k) {
+      int kp = c.kplus[(size_t)k * nk + q];
+      int km = c.kminus[(size_t)k * nk + q];
+      pp[(size_t)q * nk + k] = ((int64_t)k * nk + kp) * pe;   // V(k, k+q)
+      pm[(size_t)q * nk + k] = ((int64_t)k * nk + km) * pe;   // V(k, k-q)
+      gp[(size_t)q * nk + k] = (int64_t)kp * ge;              // G(., ., k+q)
+      gm[(size_t)q * nk + k] = (int64_t)km * ge;              // G(., ., k-q)
+      for (int s = 0; s < ns; ++s) ppns[((size_t)q * nk + k) * ns + s] = pp[(size_t)q * nk + k];
+    }
+  c.tab_pair_plus.upload(pp.data(), pp.size(), c.stream);
+  c.tab_pair_minus.upload(pm.data(), pm.size(), c.stream);
+  c.tab_g_plus.upload(gp.data(), gp.size(), c.stream);
+  c.tab_g_minus.upload(gm.data(), gm.size(), c.stream);
+  c.tab_pair_plus_ns.upload(ppns.data(), ppns.size(), c.stream);
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+void build_hf_tables(Context& c) {
+  const int nk = c.d.nk, ns = c.d.ns;
+  const int64_t pe = c.pair_elems();
+  std::vector<int64_t> dns((size_t)nk * ns);
+  for (int k = 0; k < nk; ++k)
+    for (int s = 0; s < ns; ++s) dns[(size_t)k * ns + s] = ((int64_t)k * nk + k) * pe;  // pair (k,k)
+  c.tab_pair_diag_ns.upload(dns.data(), dns.size(), c.stream);
+  GB_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+// Choose the k-block size so that the two largest intermediates fit the budget.
+static int choose_kblock(const Context& c, int64_t elems_per_k) {
+  size_t free_b = 0, total_b = 0;
+  GB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  // leave headroom; at most 24 GB for the GW intermediates
+  double budget = std::min<double>(24e9, 0.6 * (double)free_b);
+  double per_k = 2.0 * (double)elems_per_k * sizeof(cplx);
+  int kb = (int)std::max(1.0, std::floor(budget / per_k));
+  return std::min(kb, c.d.nk);
+}
+
+void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
+  const gb200_dims& d = c.d;
+  require(d.nts % 2 == 0, GB200_ERR_WRONG_GRID, "Number of tau points should be even!!!");
+  require(c.have_kq && c.have_grid && c.have_V, GB200_ERR_STATE, "gw_sigma: k/q maps, grid and integrals must be set");
+  const int nk = d.nk, ns = d.ns, nts = d.nts, nth = nts / 2, NQ = d.NQ, nw_b = d.nw_b;
+  const int64_t nao = d.nao, nao2 = nao * nao;
+  const int64_t pe = c.pair_elems();
+  const int64_t ge = nao2;                         // one G matrix
+  const int64_t g_s = (int64_t)nk * ge;            // stride of spin in G
+  const int64_t g_t = (int64_t)ns * g_s;           // stride of tau in G
+  const double pref = (ns == 2) ? 1.0 : 2.0;       // gw_cpu_kernel.cpp:167 (no X2C)
+  const bool split = c.prec_mode == GB200_PREC_SPLIT;
+
+  for (int i = 0; i < 5; ++i)
+    if (!c.ev[i]) GB_CUDA(cudaEventCreate(&c.ev[i]));
+  GB_CUDA(cudaEventRecord(c.ev[0], st));
+
+  GB_CUDA(cudaMemsetAsync(Sigma, 0, c.g_elems() * sizeof(cplx), st));
+  const int64_t per_k_sigma = (int64_t)nts * ns * pe;
+  const int kb = choose_kblock(c, per_k_sigma);
+  cplx* P0 = (cplx*)c.scratch.get(SL_P0, (size_t)nts * NQ * NQ * sizeof(cplx));
+  cplx* Pw = (cplx*)c.scratch.get(SL_PW, (size_t)nw_b * NQ * NQ * sizeof(cplx));
+  cplx* Pinv = (cplx*)c.scratch.get(SL_PINV, (size_t)nw_b * NQ * NQ * sizeof(cplx));
+  cplx* aug = (cplx*)c.scratch.get(SL_AUG, (size_t)nw_b * NQ * 2 * NQ * sizeof(cplx));
+  cplx* X1 = (cplx*)c.scratch.get(SL_Y1, (size_t)kb * per_k_sigma * sizeof(cplx));
+  cplx* X2 = (cplx*)c.scratch.get(SL_Y2, (size_t)kb * per_k_sigma * sizeof(cplx));
+  SplitEngine* se = split ? split_engine(c) : nullptr;
+  if (se) split_prepare_integrals(c, *se, st);
+  // the P0 and Sigma contractions run in the selected precision; the
+  // transforms and the aux-basis solve always run in FP64
+  auto contract = [&](const ZGemm& g) {
+    if (se) split_gemm(c, *se, g, st);
+    else zgemm_fp64(g, st);
+  };
+
+  float t_p0 = 0, t_w = 0, t_sig = 0;
+  for (int q = 0; q < nk; ++q) {
+    // ---------------- polarization P0(tau, q), tau in the first half ---------
+    GB_CUDA(cudaEventRecord(c.ev[1], st));
+    GB_CUDA(cudaMemsetAsync(P0, 0, (size_t)nts * NQ * NQ * sizeof(cplx), st));
+    for (int k0 = 0; k0 < nk; k0 += kb) {
+      const int kbk = std::min(kb, nk - k0);
+      const int64_t* tVp = c.tab_pair_plus.get() + (int64_t)q * nk + k0;
+      const int64_t* tGp = c.tab_g_plus.get() + (int64_t)q * nk + k0;
+      const int64_t blkT1 = (int64_t)nth * ns * pe;  // per kk in T1
+      // (a) T1[kk][t][s][(Q,p)][n] = sum_m V(k,k+q)[(Q,p)][m] G(t,s,k+q)[m][n]
+      ZGemm a;
+      a.M = (int64_t)NQ * nao; a.N = nao; a.K = nao;
+      a.nb0 = kbk; a.nb1 = nth; a.nb2 = ns;
+      a.A = dense(c.V.get(), nao); a.A.bat.tab0 = tVp;
+      a.B = dense(G, nao); a.B.bat.tab0 = tGp; a.B.bat.s1 = g_t; a.B.bat.s2 = g_s;
+      a.C.ptr = X1; a.C.row = lin(nao); a.C.col = lin(1);
+      a.C.bat.s0 = blkT1; a.C.bat.s1 = (int64_t)ns * pe; a.C.bat.s2 = pe;
+      // (b) Bt[t][kk][s][Q][r][n] = sum_p Gbar(nts-1-t, s, k)[r][p] T1[kk][t][s][Q][p][n]
+      ZGemm b;
+      b.M = nao; b.N = (int64_t)NQ * nao; b.K = nao;
+      b.nb0 = kbk; b.nb1 = nth; b.nb2 = ns;
+      b.A = dense(G + (int64_t)(nts - 1) * g_t + (int64_t)k0 * ge, nao);
+      b.A.bat.s0 = ge; b.A.bat.s1 = -g_t; b.A.bat.s2 = g_s;
+      b.B.ptr = X1; b.B.row = lin(nao); b.B.col = two(nao, 1, nao2);
+      b.B.bat.s0 = blkT1; b.B.bat.s1 = (int64_t)ns * pe; b.B.bat.s2 = pe;
+      b.C.ptr = X2; b.C.row = lin(nao); b.C.col = two(nao, 1, nao2);
+      b.C.bat.s0 = (int64_t)ns * pe; b.C.bat.s1 = (int64_t)kbk * ns * pe; b.C.bat.s2 = pe;
+      // (c) P0[t][Q][Q'] -= pref sum_{(kk,s),(r,n)} Bt[t][(kk,s)][Q][(r,n)] conj(V(k,k+q)[Q'][(r,n)])
+      ZGemm cc;
+      cc.M = NQ; cc.N = NQ; cc.K = (int64_t)kbk * ns * nao2;
+      cc.nb0 = 1; cc.nb1 = 1; cc.nb2 = nth;
+      cc.A.ptr = X2; cc.A.row = lin(nao2); cc.A.col = two(nao2, 1, (int64_t)NQ * nao2);
+      cc.A.bat.s2 = (int64_t)kbk * ns * pe;
+      cc.B.ptr = c.V.get(); cc.B.row = twotab(nao2, 1, c.tab_pair_plus_ns.get() + ((int64_t)q * nk + k0) * ns);
+      cc.B.col = lin(nao2); cc.B.conj = true;
+      cc.C.ptr = P0; cc.C.row = lin(NQ); cc.C.col = lin(1); cc.C.bat.s2 = (int64_t)NQ * NQ;
+      cc.alpha = cmk(-pref, 0.0); cc.beta = cmk(1.0, 0.0);
+      contract(a);
+      contract(b);
+      contract(cc);
+    }
+    {
+      int64_t total = (int64_t)nth * NQ * (NQ + 1) / 2;
+      symmetrize_p0_kernel<<<grid_for(total, 256), 256, 0, st>>>(P0, nts, NQ, 1.0 / nk);
+      GB_CHECK_LAUNCH();
+    }
+    GB_CUDA(cudaEventRecord(c.ev[2], st));
+    // ---------------- screened interaction (gw_cpu_kernel.cpp:227-279) -------
+    {
+      ZGemm f;  // Pw[n] = sum_t Tnt_b[n][t] P0[t]
+      f.M = nw_b; f.N = (int64_t)NQ * NQ; f.K = nts;
+      f.A = dense(c.Tnt_b.get(), nts);
+      f.B = dense(P0, (int64_t)NQ * NQ);
+      f.C.ptr = Pw; f.C.row = lin((int64_t)NQ * NQ); f.C.col = lin(1);
+      zgemm_fp64(f, st);
+      // temp = LDLT(I - Pw)^-1 on the lower triangle, then hermitize
+      invert_large_batched(Pw, Pinv, aug, nw_b, NQ, true, true, st);
+      hermitize_batched(Pinv, nw_b, NQ, 1.0, st);
+      ZGemm m;  // Pw[n] <- temp[n] Pw[n] (written to aug as scratch, then used)
+      m.M = NQ; m.N = NQ; m.K = NQ; m.nb2 = nw_b;
+      m.A = dense(Pinv, NQ); m.A.bat.s2 = (int64_t)NQ * NQ;
+      m.B = dense(Pw, NQ); m.B.bat.s2 = (int64_t)NQ * NQ;
+      m.C.ptr = aug; m.C.row = lin(NQ); m.C.col = lin(1); m.C.bat.s2 = (int64_t)NQ * NQ;
+      zgemm_fp64(m, st);
+      ZGemm bt;  // W(tau) = sum_n Ttn_b[t][n] P(i Omega_n) -> stored in P0
+      bt.M = nts; bt.N = (int64_t)NQ * NQ; bt.K = nw_b;
+      bt.A = dense(c.Ttn_b.get(), nw_b);
+      bt.B = dense(aug, (int64_t)NQ * NQ);
+      bt.C.ptr = P0; bt.C.row = lin((int64_t)NQ * NQ); bt.C.col = lin(1);
+      zgemm_fp64(bt, st);
+    }
+    GB_CUDA(cudaEventRecord(c.ev[3], st));
+    // ---------------- self-energy contribution of this q ---------------------
+    for (int k0 = 0; k0 < nk; k0 += kb) {
+      const int kbk = std::min(kb, nk - k0);
+      const int64_t* tVm = c.tab_pair_minus.get() + (int64_t)q * nk + k0;
+      const int64_t* tGm = c.tab_g_minus.get() + (int64_t)q * nk + k0;
+      const int64_t blk = (int64_t)nts * ns * pe;  // per kk in Y1 / Y2
+      // (d) Y1[kk][t][s][(Q,i)][n] = sum_m V(k,k-q)[(Q,i)][m] G(t,s,k-q)[m][n]
+      ZGemm dd;
+      dd.M = (int64_t)NQ * nao; dd.N = nao; dd.K = nao;
+      dd.nb0 = kbk; dd.nb1 = nts; dd.nb2 = ns;
+      dd.A = dense(c.V.get(), nao); dd.A.bat.tab0 = tVm;
+      dd.B = dense(G, nao); dd.B.bat.tab0 = tGm; dd.B.bat.s1 = g_t; dd.B.bat.s2 = g_s;
+      dd.C.ptr = X1; dd.C.row = lin(nao); dd.C.col = lin(1);
+      dd.C.bat.s0 = blk; dd.C.bat.s1 = (int64_t)ns * pe; dd.C.bat.s2 = pe;
+      // (e) Y2[kk][t][s][(i,n)][Q'] = sum_Q Y1[kk][t][s][Q][(i,n)] W(t)[Q][Q']
+      ZGemm e;
+      e.M = (int64_t)kbk * nao2; e.N = NQ; e.K = NQ;
+      e.nb0 = 1; e.nb1 = nts; e.nb2 = ns;
+      e.A.ptr = X1; e.A.row = two(nao2, 1, blk); e.A.col = lin(nao2);
+      e.A.bat.s1 = (int64_t)ns * pe; e.A.bat.s2 = pe;
+      e.B = dense(P0, NQ); e.B.bat.s1 = (int64_t)NQ * NQ;
+      e.C.ptr = X2; e.C.row = two(nao2, NQ, blk); e.C.col = lin(1);
+      e.C.bat.s1 = (int64_t)ns * pe; e.C.bat.s2 = pe;
+      // (f) Sigma[t][s][k][i][j] -= sum_{(n,Q')} Y2[kk][t][s][i][(n,Q')] conj(V(k,k-q)[Q'][j][n])
+      ZGemm f;
+      f.M = nao; f.N = nao; f.K = nao * NQ;
+      f.nb0 = kbk; f.nb1 = nts; f.nb2 = ns;
+      f.A.ptr = X2; f.A.row = lin(nao * NQ); f.A.col = lin(1);
+      f.A.bat.s0 = blk; f.A.bat.s1 = (int64_t)ns * pe; f.A.bat.s2 = pe;
+      f.B.ptr = c.V.get(); f.B.row = two(NQ, nao2, 1); f.B.col = lin(nao); f.B.conj = true;
+      f.B.bat.tab0 = tVm;
+      f.C.ptr = Sigma + (int64_t)k0 * ge; f.C.row = lin(nao); f.C.col = lin(1);
+      f.C.bat.s0 = ge; f.C.bat.s1 = g_t; f.C.bat.s2 = g_s;
+      f.alpha = cmk(-1.0, 0.0); f.beta = cmk(1.0, 0.0);
+      contract(dd);
+      contract(e);
+      contract(f);
+    }
+    GB_CUDA(cudaEventRecord(c.ev[4], st));
+    GB_CUDA(cudaEventSynchronize(c.ev[4]));
+    float a_ms = 0, b_ms = 0, c_ms = 0;
+    GB_CUDA(cudaEventElapsedTime(&a_ms, c.ev[1], c.ev[2]));
+    GB_CUDA(cudaEventElapsedTime(&b_ms, c.ev[2], c.ev[3]));
+    GB_CUDA(cudaEventElapsedTime(&c_ms, c.ev[3], c.ev[4]));
+    t_p0 += a_ms; t_w += b_ms; t_sig += c_ms;
+  }
+  scale_inplace(Sigma, c.g_elems(), 1.0 / nk, st);  // gw_cpu_kernel.cpp:55
+  GB_CUDA(cudaEventRecord(c.ev[4], st));
+  GB_CUDA(cudaEventSynchronize(c.ev[4]));
+  float tot = 0;
+  GB_CUDA(cudaEventElapsedTime(&tot, c.ev[0], c.ev[4]));
+  c.timings[0] = t_p0; c.timings[1] = t_w; c.timings[2] = t_sig; c.timings[3] = tot;
+}
+
+}  // namespace gb200

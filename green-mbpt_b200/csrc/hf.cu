@@ -1,0 +1,125 @@
+// Hartree-Fock Fock matrix on one GPU (hf_scalar_cpu_kernel::solve,
+// green-mbpt src/hf_cpu_kernels.cpp:25-146) for the no-symmetry case.
+//
+//   J: u_Q = (1/nk) sum_{k,s} sum_ab V^Q_ab(k,k) dm_ba(k,s);  F_ij(k,s) = sum_Q u_Q V^Q_ij(k,k)
+//   K: F_ij(k,s) -= (c/nk) sum_{k'} sum_{Q,a} Y^Q_ia conj(V^Q_ja(k,k')),
+//      Y^Q = V^Q(k,k') dm(k',s), c = 0.5 (ns = 1) or 1
+//   Madelung: F -= c * madelung * S dm S
+#include <algorithm>
+
+#include "context.cuh"
+
+namespace gb200 {
+namespace {
+
+// dmT[k][s][a][b] = dm[s][k][b][a]
+__global__ void dm_transpose_kernel(const cplx* dm, cplx* dmT, int ns, int nk, int n) {
+  const int64_t total = (int64_t)ns * nk * n * n;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t m = e / ((int64_t)n * n);
+    int r = (int)(e % ((int64_t)n * n));
+    int a = r / n, b = r % n;
+    int s = (int)(m / nk), k = (int)(m % nk);
+    dmT[(((int64_t)k * ns + s) * n + a) * n + b] = dm[e - r + (int64_t)b * n + a];
+  }
+}
+
+ZOperand dense(const cplx* p, int64_t ld) {
+  ZOperand o;
+  o.ptr = p;
+  o.row = lin(ld);
+  o.col = lin(1);
+  return o;
+}
+
+}  // namespace
+
+void hf_fock(Context& c, const cplx* dm, const cplx* S, double madelung, cplx* F, cudaStream_t st) {
+  const gb200_dims& d = c.d;
+  require(c.have_Vhf || c.have_V, GB200_ERR_STATE, "hf_fock: integrals not set");
+  const cplx* V = c.have_Vhf ? c.Vhf.get() : c.V.get();
+  if (!c.tab_pair_diag_ns.get()) build_hf_tables(c);
+  const int nk = d.nk, ns = d.ns, NQ = d.NQ;
+  const int64_t nao = d.nao, nao2 = nao * nao, pe = c.pair_elems();
+  const double pref = (ns == 2) ? 1.0 : 0.5;  // hf_cpu_kernels.cpp:98
+
+  // ---- direct (Hartree) term ----
+  cplx* dmT = (cplx*)c.scratch.get(SL_HF_DMT, (size_t)ns * nk * nao2 * sizeof(cplx));
+  cplx* u = (cplx*)c.scratch.get(SL_HF_U, (size_t)NQ * sizeof(cplx));
+  {
+    int64_t total = (int64_t)ns * nk * nao2;
+    unsigned g = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 16);
+    dm_transpose_kernel<<<std::max(1u, g), 256, 0, st>>>(dm, dmT, ns, nk, (int)nao);
+    GB_CHECK_LAUNCH();
+  }
+  {
+    ZGemm g;  // u[Q] = (1/nk) sum_{(k,s),(a,b)} V(k,k)[Q][a][b] dmT[(k,s)][a][b]
+    g.M = NQ; g.N = 1; g.K = (int64_t)nk * ns * nao2;
+    g.A.ptr = V; g.A.row = lin(nao2); g.A.col = twotab(nao2, 1, c.tab_pair_diag_ns.get());
+    g.B.ptr = dmT; g.B.row = lin(1); g.B.col = lin(0);
+    g.C.ptr = u; g.C.row = lin(1); g.C.col = lin(0);
+    g.alpha = cmk(1.0 / nk, 0.0);
+    zgemm_fp64(g, st);
+  }
+  {
+    ZGemm g;  // F[s][k][(i,j)] = sum_Q u[Q] V(k,k)[Q][(i,j)]
+    g.M = 1; g.N = nao2; g.K = NQ;
+    g.nb0 = nk; g.nb2 = ns;
+    g.A.ptr = u; g.A.row = lin(0); g.A.col = lin(1);
+    g.B.ptr = V; g.B.row = lin(nao2); g.B.col = lin(1);
+    g.B.bat.s0 = ((int64_t)nk + 1) * pe;  // pair (k,k) of the full [nk][nk] storage
+    g.C.ptr = F; g.C.row = lin(0); g.C.col = lin(1);
+    g.C.bat.s0 = nao2; g.C.bat.s2 = (int64_t)nk * nao2;
+    zgemm_fp64(g, st);
+  }
+  // ---- exchange term, blocked over k ----
+  const int64_t per_k = (int64_t)ns * nk * pe;
+  size_t free_b = 0, total_b = 0;
+  GB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  double budget = std::min<double>(8e9, 0.5 * (double)free_b);
+  int kb = (int)std::max(1.0, std::floor(budget / ((double)per_k * sizeof(cplx))));
+  kb = std::min(kb, nk);
+  cplx* Y = (cplx*)c.scratch.get(SL_HF_Y, (size_t)kb * per_k * sizeof(cplx));
+  for (int k0 = 0; k0 < nk; k0 += kb) {
+    const int kbk = std::min(kb, nk - k0);
+    ZGemm y;  // Y[kk][s][k'][(Q,i)][a] = sum_b V(k,k')[(Q,i)][b] dm[s][k'][b][a]
+    y.M = (int64_t)NQ * nao; y.N = nao; y.K = nao;
+    y.nb0 = kbk; y.nb1 = ns; y.nb2 = nk;
+    y.A = dense(V + (int64_t)k0 * nk * pe, nao);
+    y.A.bat.s0 = (int64_t)nk * pe; y.A.bat.s2 = pe;
+    y.B = dense(dm, nao); y.B.bat.s1 = (int64_t)nk * nao2; y.B.bat.s2 = nao2;
+    y.C.ptr = Y; y.C.row = lin(nao); y.C.col = lin(1);
+    y.C.bat.s0 = per_k; y.C.bat.s1 = (int64_t)nk * pe; y.C.bat.s2 = pe;
+    zgemm_fp64(y, st);
+    ZGemm x;  // F[s][k][i][j] -= (c/nk) sum_{(k',Q),a} Y[kk][s][(k',Q)][i][a] conj(V(k,k')[(k',Q)][j][a])
+    x.M = nao; x.N = nao; x.K = (int64_t)nk * NQ * nao;
+    x.nb0 = kbk; x.nb2 = ns;
+    x.A.ptr = Y; x.A.row = lin(nao); x.A.col = two(nao, 1, nao2);
+    x.A.bat.s0 = per_k; x.A.bat.s2 = (int64_t)nk * pe;
+    x.B.ptr = V + (int64_t)k0 * nk * pe; x.B.row = two(nao, 1, nao2); x.B.col = lin(nao); x.B.conj = true;
+    x.B.bat.s0 = (int64_t)nk * pe;
+    x.C.ptr = F + (int64_t)k0 * nao2; x.C.row = lin(nao); x.C.col = lin(1);
+    x.C.bat.s0 = nao2; x.C.bat.s2 = (int64_t)nk * nao2;
+    x.alpha = cmk(-pref / nk, 0.0); x.beta = cmk(1.0, 0.0);
+    zgemm_fp64(x, st);
+  }
+  // ---- Madelung / Ewald term ----
+  if (madelung != 0.0) {
+    cplx* T = (cplx*)c.scratch.get(SL_TMP, (size_t)ns * nk * nao2 * sizeof(cplx));
+    ZGemm a;  // T = S dm
+    a.M = nao; a.N = nao; a.K = nao; a.nb2 = (int64_t)ns * nk;
+    a.A = dense(S, nao); a.A.bat.s2 = nao2;
+    a.B = dense(dm, nao); a.B.bat.s2 = nao2;
+    a.C.ptr = T; a.C.row = lin(nao); a.C.col = lin(1); a.C.bat.s2 = nao2;
+    zgemm_fp64(a, st);
+    ZGemm b;  // F -= c * madelung * T S
+    b.M = nao; b.N = nao; b.K = nao; b.nb2 = (int64_t)ns * nk;
+    b.A = dense(T, nao); b.A.bat.s2 = nao2;
+    b.B = dense(S, nao); b.B.bat.s2 = nao2;
+    b.C.ptr = F; b.C.row = lin(nao); b.C.col = lin(1); b.C.bat.s2 = nao2;
+    b.alpha = cmk(-pref * madelung, 0.0); b.beta = cmk(1.0, 0.0);
+    zgemm_fp64(b, st);
+  }
+}
+
+}  // namespace gb200

@@ -1,0 +1,234 @@
+// FP64 batched linear algebra: hermitization and Gauss-Jordan inverses.
+//
+// Small matrices (n <= 64, the Dyson inverses of nso x nso) live entirely in
+// shared memory, one CTA per matrix.  Large ones (the NQ x NQ aux-basis
+// matrices of the screened interaction) keep the augmented [A | I] in a
+// global scratch buffer that stays resident in L2; one CTA per matrix walks
+// the pivot columns.  Both use partial (row) pivoting.
+#include "context.cuh"
+
+namespace gb200 {
+namespace {
+
+__global__ void hermitize_kernel(cplx* X, int64_t nmat, int n, double scale) {
+  const int64_t npairs = (int64_t)n * (n + 1) / 2;
+  const int64_t total = nmat * npairs;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t m = e / npairs;
+    int64_t p = e - m * npairs;
+    // p -> (i, j) with i >= j
+    int i = (int)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
+    while ((int64_t)i * (i + 1) / 2 > p) --i;
+    while ((int64_t)(i + 1) * (i + 2) / 2 <= p) ++i;
+    int j = (int)(p - (int64_t)i * (i + 1) / 2);
+    cplx* M = X + m * (int64_t)n * n;
+    cplx a = cscale(M[(int64_t)i * n + j], scale);
+    cplx b = cscale(M[(int64_t)j * n + i], scale);
+    cplx h = cscale(cadd(a, cconj(b)), 0.5);
+    M[(int64_t)i * n + j] = h;
+    M[(int64_t)j * n + i] = cconj(h);
+  }
+}
+
+__global__ void scale_kernel(cplx* X, int64_t count, double s) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < count; e += (int64_t)gridDim.x * blockDim.x) {
+    X[e] = cscale(X[e], s);
+  }
+}
+
+__device__ __forceinline__ cplx crecip(cplx a) {
+  double d = a.x * a.x + a.y * a.y;
+  return make_double2(a.x / d, -a.y / d);
+}
+
+// Block-wide argmax of |aug[i][j]|^2 over i in [j, n).
+template <int NT>
+__device__ int pivot_search(const cplx* aug, int64_t ld, int j, int n, double* sval, int* sidx) {
+  double best = -1.0;
+  int bi = j;
+  for (int i = j + threadIdx.x; i < n; i += NT) {
+    double v = cabs2(aug[(int64_t)i * ld + j]);
+    if (v > best) { best = v; bi = i; }
+  }
+  sval[threadIdx.x] = best;
+  sidx[threadIdx.x] = bi;
+  __syncthreads();
+  for (int s = NT / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      double o = sval[threadIdx.x + s];
+      int oi = sidx[threadIdx.x + s];
+      if (o > sval[threadIdx.x] || (o == sval[threadIdx.x] && oi < sidx[threadIdx.x])) {
+        sval[threadIdx.x] = o;
+        sidx[threadIdx.x] = oi;
+      }
+    }
+    __syncthreads();
+  }
+  int p = sidx[0];
+  __syncthreads();
+  return p;
+}
+
+constexpr int SMALL_NT = 256;
+
+__global__ void __launch_bounds__(SMALL_NT) invert_small_kernel(const cplx* A, cplx* Ainv, int n) {
+  extern __shared__ double2 smem_c[];
+  cplx* aug = smem_c;                 // n x 2n
+  cplx* fac = aug + 2 * n * n;        // n
+  __shared__ double sval[SMALL_NT];
+  __shared__ int sidx[SMALL_NT];
+  const int64_t m = blockIdx.x;
+  const cplx* Am = A + m * (int64_t)n * n;
+  const int ld = 2 * n;
+  for (int e = threadIdx.x; e < n * n; e += SMALL_NT) {
+    int i = e / n, c = e % n;
+    aug[i * ld + c] = Am[e];
+    aug[i * ld + n + c] = (i == c) ? cmk(1.0, 0.0) : cmk(0.0, 0.0);
+  }
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    int p = pivot_search<SMALL_NT>(aug, ld, j, n, sval, sidx);
+    if (p != j) {
+      for (int c = threadIdx.x; c < ld; c += SMALL_NT) {
+        cplx t = aug[j * ld + c];
+        aug[j * ld + c] = aug[p * ld + c];
+        aug[p * ld + c] = t;
+      }
+      __syncthreads();
+    }
+    cplx inv = crecip(aug[j * ld + j]);
+    __syncthreads();
+    for (int c = threadIdx.x; c < ld; c += SMALL_NT) aug[j * ld + c] = cmul(aug[j * ld + c], inv);
+    for (int i = threadIdx.x; i < n; i += SMALL_NT) fac[i] = aug[i * ld + j];
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * (ld - j); e += SMALL_NT) {
+      int i = e / (ld - j), c = j + e % (ld - j);
+      if (i == j) continue;
+      aug[i * ld + c] = csub(aug[i * ld + c], cmul(fac[i], aug[j * ld + c]));
+    }
+    __syncthreads();
+  }
+  cplx* Om = Ainv + m * (int64_t)n * n;
+  for (int e = threadIdx.x; e < n * n; e += SMALL_NT) {
+    int i = e / n, c = e % n;
+    Om[e] = aug[i * ld + n + c];
+  }
+}
+
+constexpr int LARGE_NT = 1024;
+
+__global__ void __launch_bounds__(LARGE_NT) invert_large_kernel(const cplx* A, cplx* Ainv, cplx* augbase, int n,
+                                                                 bool herm_from_lower, bool identity_minus) {
+  extern __shared__ double2 smem_c[];
+  cplx* prow = smem_c;           // 2n (pivot row)
+  cplx* fac = prow + 2 * n;      // n
+  __shared__ double sval[LARGE_NT];
+  __shared__ int sidx[LARGE_NT];
+  const int64_t m = blockIdx.x;
+  const int ld = 2 * n;
+  cplx* aug = augbase + m * (int64_t)n * ld;
+  const cplx* Am = A + m * (int64_t)n * n;
+  for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += LARGE_NT) {
+    int i = (int)(e / n), c = (int)(e % n);
+    // B = identity_minus ? I - A : A ; the inverted matrix is B itself or, with
+    // herm_from_lower, the Hermitian matrix of B's strict lower triangle and
+    // real diagonal (what Eigen's LDLT reads, gw_cpu_kernel.cpp:245-249)
+    auto Bel = [&](int x, int y) -> cplx {
+      cplx a = Am[(int64_t)x * n + y];
+      return identity_minus ? cmk((x == y ? 1.0 : 0.0) - a.x, -a.y) : a;
+    };
+    cplx v;
+    if (herm_from_lower) {
+      if (i > c) v = Bel(i, c);
+      else if (i < c) v = cconj(Bel(c, i));
+      else v = cmk(Bel(i, i).x, 0.0);
+    } else {
+      v = Bel(i, c);
+    }
+    aug[(int64_t)i * ld + c] = v;
+    aug[(int64_t)i * ld + n + c] = (i == c) ? cmk(1.0, 0.0) : cmk(0.0, 0.0);
+  }
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    int p = pivot_search<LARGE_NT>(aug, ld, j, n, sval, sidx);
+    if (p != j) {
+      for (int c = threadIdx.x; c < ld; c += LARGE_NT) {
+        cplx t = aug[(int64_t)j * ld + c];
+        aug[(int64_t)j * ld + c] = aug[(int64_t)p * ld + c];
+        aug[(int64_t)p * ld + c] = t;
+      }
+      __syncthreads();
+    }
+    cplx inv = crecip(aug[(int64_t)j * ld + j]);
+    for (int c = threadIdx.x; c < ld; c += LARGE_NT) prow[c] = cmul(aug[(int64_t)j * ld + c], inv);
+    for (int i = threadIdx.x; i < n; i += LARGE_NT) fac[i] = aug[(int64_t)i * ld + j];
+    __syncthreads();
+    for (int c = threadIdx.x; c < ld; c += LARGE_NT) aug[(int64_t)j * ld + c] = prow[c];
+    const int w = ld - j;
+    for (int64_t e = threadIdx.x; e < (int64_t)n * w; e += LARGE_NT) {
+      int i = (int)(e / w), c = j + (int)(e % w);
+      if (i == j) continue;
+      aug[(int64_t)i * ld + c] = csub(aug[(int64_t)i * ld + c], cmul(fac[i], prow[c]));
+    }
+    __syncthreads();
+  }
+  cplx* Om = Ainv + m * (int64_t)n * n;
+  for (int64_t e = threadIdx.x; e < (int64_t)n * n; e += LARGE_NT) {
+    int i = (int)(e / n), c = (int)(e % n);
+    Om[e] = aug[(int64_t)i * ld + n + c];
+  }
+}
+
+inline unsigned grid_for(int64_t n, int nt) {
+  int64_t g = (n + nt - 1) / nt;
+  if (g > 148 * 32) g = 148 * 32;
+  if (g < 1) g = 1;
+  return (unsigned)g;
+}
+
+}  // namespace
+
+void hermitize_batched(cplx* X, int64_t nmat, int n, double scale, cudaStream_t st) {
+  if (nmat <= 0) return;
+  int64_t total = nmat * (int64_t)n * (n + 1) / 2;
+  hermitize_kernel<<<grid_for(total, 256), 256, 0, st>>>(X, nmat, n, scale);
+  GB_CHECK_LAUNCH();
+}
+
+void scale_inplace(cplx* X, int64_t count, double s, cudaStream_t st) {
+  if (count <= 0) return;
+  scale_kernel<<<grid_for(count, 256), 256, 0, st>>>(X, count, s);
+  GB_CHECK_LAUNCH();
+}
+
+void invert_small_batched(const cplx* A, cplx* Ainv, int64_t nmat, int n, cudaStream_t st) {
+  require(n <= 64, GB200_ERR_INVALID, "invert_small_batched: n > 64");
+  if (nmat <= 0) return;
+  size_t smem = (size_t)(2 * n * n + n) * sizeof(cplx);
+  static bool attr_set = false;
+  if (!attr_set) {
+    GB_CUDA(cudaFuncSetAttribute(invert_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr_set = true;
+  }
+  for (int64_t off = 0; off < nmat; off += 2147483647LL) {
+    int64_t cnt = nmat - off < 2147483647LL ? nmat - off : 2147483647LL;
+    invert_small_kernel<<<(unsigned)cnt, SMALL_NT, smem, st>>>(A + off * n * n, Ainv + off * n * n, n);
+    GB_CHECK_LAUNCH();
+  }
+}
+
+void invert_large_batched(const cplx* A, cplx* Ainv, cplx* aug, int64_t nmat, int n, bool herm_from_lower,
+                          bool identity_minus, cudaStream_t st) {
+  require(n <= 4096, GB200_ERR_INVALID, "invert_large_batched: n > 4096");
+  if (nmat <= 0) return;
+  size_t smem = (size_t)(3 * n) * sizeof(cplx);
+  static bool attr_set = false;
+  if (!attr_set) {
+    GB_CUDA(cudaFuncSetAttribute(invert_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    attr_set = true;
+  }
+  invert_large_kernel<<<(unsigned)nmat, LARGE_NT, smem, st>>>(A, Ainv, aug, n, herm_from_lower, identity_minus);
+  GB_CHECK_LAUNCH();
+}
+
+}  // namespace gb200

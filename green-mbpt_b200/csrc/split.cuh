@@ -1,0 +1,21 @@
+// Split-precision (Ozaki-sliced INT8 tensor-core) contractions.
+#pragma once
+
+#include "context.cuh"
+
+namespace gb200 {
+
+struct SplitEngine;
+
+// The engine of a context (created on first use).
+SplitEngine* split_engine(Context& c);
+// Prepare per-integral data (no-op when nothing is cached).
+void split_prepare_integrals(Context& c, SplitEngine& se, cudaStream_t st);
+// C = alpha op(A) op(B) + beta C with both operands sliced into INT8 pieces,
+// products on the tensor cores with exact INT32 accumulation, FP64 recombination.
+void split_gemm(Context& c, SplitEngine& se, const ZGemm& g, cudaStream_t st);
+// Drop cached slices (integrals or precision changed).
+void split_invalidate(Context& c);
+void split_release(Context& c);
+
+}  // namespace gb200

@@ -1,0 +1,99 @@
+"""Host-side mirror of green-mbpt's solver interface on top of the C ABI.
+
+The reference wires its kernels as
+  gw_solver(p, ft, bz, S_k).solve(G, Sigma1, Sigma_tau)   (gw_solver.h:61-72, gw_solver.cpp:30-32)
+  hf_solver(p, bz, S_k).solve(G, Sigma1, Sigma_tau)       (hf_solver.h:27-43, hf_solver.cpp:9-16)
+  dyson(p).solve(G, Sigma1, Sigma_tau); dyson.diff(...)   (dyson.cpp:290-317)
+These classes keep the same names, call order, argument meaning and error
+classes; the arrays are numpy complex128 with the reference's index order.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import lib
+from .synth import System
+
+
+def kq_maps(mesh):
+    """k1_from_k2q / k2_from_k1q tables of a Monkhorst-Pack mesh without symmetry."""
+    n1, n2, n3 = mesh
+    nk = n1 * n2 * n3
+    idx = np.arange(nk)
+    f = np.stack([idx // (n2 * n3), (idx // n3) % n2, idx % n3], axis=1)
+
+    def index(v):
+        v = np.mod(v, (n1, n2, n3))
+        return v[..., 0] * n2 * n3 + v[..., 1] * n3 + v[..., 2]
+
+    kplus = index(f[:, None, :] + f[None, :, :]).astype(np.int32)   # [k, q] -> k + q
+    kminus = index(f[:, None, :] - f[None, :, :]).astype(np.int32)  # [k, q] -> k - q
+    return kplus, kminus
+
+
+def make_context(system: System, device: int = 0, precision: int = lib.PREC_FP64, slices: int = 4,
+                 hf_integrals=None) -> lib.Context:
+    """Context with maps, grid, integrals and Hamiltonian of a synthetic system uploaded."""
+    g = system.grid
+    ctx = lib.Context(system.nk, system.nao, system.ns, system.NQ, g.nts, g.nw, g.nw_b, system.beta, device=device)
+    kp, km = kq_maps(system.mesh)
+    ctx.set_kq_maps(kp, km)
+    ctx.set_grid(g.Tnt_f, g.Ttn_f, g.Tnt_b, g.Ttn_b, g.wsample_f)
+    ctx.set_integrals(system.V_half, lib.INTEGRALS_GW)
+    if hf_integrals is not None:
+        ctx.set_integrals(hf_integrals, lib.INTEGRALS_HF)
+    ctx.set_hamiltonian(system.F, system.S)
+    ctx.set_precision(precision, slices)
+    return ctx
+
+
+class gw_solver:
+    """GW self-energy through the B200 kernel (custom_gw_kernel callback)."""
+
+    def __init__(self, ctx: lib.Context):
+        self.ctx = ctx
+
+    def solve(self, G, Sigma1, Sigma_tau):
+        Sigma_tau[...] = self.ctx.gw_sigma(G)
+
+
+class hf_solver:
+    """Hartree-Fock through the B200 kernel (custom_hf_kernel callback)."""
+
+    def __init__(self, ctx: lib.Context, S, madelung: float, ns: int, X2C: bool = False):
+        if ns != 1 and X2C:
+            raise ValueError('For GSCF methods, "ns" has to be 1.')
+        self.ctx = ctx
+        self.S = np.ascontiguousarray(S, dtype=np.complex128)
+        self.madelung = float(madelung)
+        self.spin_prefactor = -1.0 if (ns == 2 or X2C) else -2.0   # hf_solver.h:38
+
+    def solve(self, G, Sigma1, Sigma_tau):
+        dm = self.spin_prefactor * np.ascontiguousarray(G[-1])
+        Sigma1[...] = self.ctx.hf_fock(dm, self.S, self.madelung)
+
+
+class dyson:
+    """Dyson step: find_mu (if const_density) then compute_G; diff() returns |dE|."""
+
+    def __init__(self, ctx: lib.Context, nel: float, mu: float = 0.0, tol: float = 1e-9, const_density: bool = True):
+        self.ctx = ctx
+        self.nel = float(nel)
+        self.mu = float(mu)
+        self.tol = float(tol)
+        self.const_density = const_density
+        self.E = (0.0, 0.0, 0.0)
+
+    def solve(self, G, Sigma1, Sigma_tau):
+        if self.const_density:
+            _, self.mu = self.ctx.find_mu(Sigma1, Sigma_tau, self.mu, self.nel, self.tol)
+        Gn, S1h, Sth = self.ctx.compute_G(Sigma1, Sigma_tau, self.mu)
+        G[...] = Gn
+        Sigma1[...] = S1h
+        Sigma_tau[...] = Sth
+
+    def diff(self, G, Sigma1, Sigma_tau):
+        e = self.ctx.energy(G, Sigma1, Sigma_tau)
+        d = sum(abs(a - b) for a, b in zip(e, self.E))
+        self.E = e
+        return d

@@ -1,0 +1,140 @@
+/*
+ * gb200.h — C ABI of the B200 density-fitted GW / HF / Dyson engine.
+ *
+ * Plain C: opaque context, plain pointers and sizes, int status codes.  Complex
+ * numbers are interleaved (re, im) pairs of double, arrays are row-major with
+ * the reference's index order.  Every "host" entry point takes host pointers,
+ * copies to the GPU, computes and copies back; every "_device" entry point
+ * takes device pointers and a cudaStream_t passed as void*.
+ *
+ * The entry points replace the reference's kernel plug-in interface
+ * (green-mbpt, src/green/mbpt/kernel_factory.h:28-36,44-108):
+ *   custom_gw_kernel -> callback (G, Sigma)  ==> gb200_gw_sigma
+ *   custom_hf_kernel -> callback (dm) -> F    ==> gb200_hf_fock
+ * and the Dyson step of src/dyson.cpp (find_mu :101-174, compute_G :176-288)
+ * plus compute_energy of src/common_utils.cpp:5-55.
+ */
+#ifndef GB200_H
+#define GB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The C++ plug-in shim maps them onto the reference's
+ * exception classes (src/green/mbpt/except.h:28-56). */
+#define GB200_OK 0
+#define GB200_ERR_INVALID 1          /* bad argument or shape -> mbpt_kernel_error */
+#define GB200_ERR_WRONG_GRID 2       /* odd number of tau points -> mbpt_wrong_grid */
+#define GB200_ERR_MU_SEARCH 3        /* stalled bisection -> mbpt_chemical_potential_search_failure */
+#define GB200_ERR_OUTDATED_INPUT 4   /* integral format version too old -> mbpt_outdated_input */
+#define GB200_ERR_CUDA 5             /* CUDA runtime / launch failure -> mbpt_kernel_error */
+#define GB200_ERR_OOM 6              /* device allocation failed -> mbpt_kernel_error */
+#define GB200_ERR_STATE 7            /* required set-up call missing -> mbpt_kernel_error */
+#define GB200_ERR_NONFINITE 8        /* NaN/Inf found in a result -> mbpt_kernel_error */
+
+/* Contraction precision for the P0 and Sigma contractions. */
+#define GB200_PREC_FP64 0            /* plain FP64 (the oracle-parity path) */
+#define GB200_PREC_SPLIT 1           /* Ozaki-sliced INT8 tensor-core products, FP64 recombination */
+
+/* Which DF integral set a call refers to (dfintegral_file vs dfintegral_hf_file, common_defs.h:156-157). */
+#define GB200_INTEGRALS_GW 0
+#define GB200_INTEGRALS_HF 1
+
+typedef struct gb200_context gb200_context;
+
+/* Problem dimensions (the constructor arguments of gw_cpu_kernel / hf_kernel,
+ * src/green/mbpt/kernels.h:42-53,186-189).  No point-group symmetry: every
+ * k-point is irreducible (ink = nk). */
+typedef struct {
+  int32_t nk;      /* k-points of the full mesh */
+  int32_t nao;     /* atomic orbitals */
+  int32_t nso;     /* spin orbitals (== nao; X2C is not supported by the GPU path) */
+  int32_t ns;      /* spin channels, 1 or 2 */
+  int32_t NQ;      /* auxiliary basis size */
+  int32_t nts;     /* tau points (even) */
+  int32_t nw;      /* fermionic Matsubara samples */
+  int32_t nw_b;    /* bosonic Matsubara samples */
+  double beta;     /* inverse temperature */
+} gb200_dims;
+
+/* Library version string and the integral-format version it accepts
+ * (INPUT_VERSION, common_defs.h:35; CheckVersion :191-212). */
+const char* gb200_version(void);
+int gb200_check_integral_version(const char* version);
+
+/* Create / destroy a context bound to CUDA device `device`.
+ * Replaces the kernel object built by gw_kernel_factory::get_kernel /
+ * hf_kernel_factory::get_kernel (kernel_factory.h:44-108). */
+int gb200_create(const gb200_dims* dims, int device, gb200_context** out);
+void gb200_destroy(gb200_context* ctx);
+const char* gb200_last_error(const gb200_context* ctx);
+
+/* k/q maps of brillouin_zone_utils::k_q_map (call sites gw_cpu_kernel.cpp:90,117):
+ * kplus[k*nk+q] = k1_from_k2q(k, q), kminus[k*nk+q] = k2_from_k1q(k, q). */
+int gb200_set_kq_maps(gb200_context* ctx, const int32_t* kplus, const int32_t* kminus);
+
+/* Imaginary-time transforms of transformer_t as dense complex matrices:
+ * Tnt_f [nw,nts], Ttn_f [nts,nw], Tnt_b [nw_b,nts], Ttn_b [nts,nw_b];
+ * wsample_f [nw] fermionic frequencies (real omega_n). */
+int gb200_set_grid(gb200_context* ctx, const double* Tnt_f, const double* Ttn_f, const double* Tnt_b,
+                   const double* Ttn_b, const double* wsample_f);
+
+/* DF integrals V^Q_ij(k1,k2) in the reference's stored form: only k1 >= k2 at
+ * pair index k1*(k1+1)/2 + k2, shape [nk(nk+1)/2, NQ, nao, nao]
+ * (df_integral_t.h:64-92,162-177).  `which` = GB200_INTEGRALS_GW / _HF. */
+int gb200_set_integrals(gb200_context* ctx, int which, const double* V_half, int64_t npairs);
+
+/* Contraction precision (GB200_PREC_*) and, for GB200_PREC_SPLIT, the number
+ * of INT8 slices per operand (2..8). */
+int gb200_set_precision(gb200_context* ctx, int mode, int slices);
+
+/* GW self-energy: Sigma(tau,k) from G(tau,k), both [nts, ns, nk, nso, nso].
+ * Replaces gw_cpu_kernel::solve (gw_cpu_kernel.cpp:31-72): Sigma is zeroed,
+ * accumulated over q and divided by nk. */
+int gb200_gw_sigma(gb200_context* ctx, const double* G, double* Sigma);
+int gb200_gw_sigma_device(gb200_context* ctx, const double* G_dev, double* Sigma_dev, void* stream);
+
+/* Hartree-Fock Fock matrix F [ns, nk, nso, nso] from the density matrix dm
+ * and overlap S (same shape).  Replaces hf_scalar_cpu_kernel::solve
+ * (hf_cpu_kernels.cpp:25-146); dm = spin_prefactor * G(beta) as in
+ * hf_solver::solve (hf_solver.cpp:9-16). */
+int gb200_hf_fock(gb200_context* ctx, const double* dm, const double* S, double madelung, double* F);
+int gb200_hf_fock_device(gb200_context* ctx, const double* dm_dev, const double* S_dev, double madelung,
+                         double* F_dev, void* stream);
+
+/* Dyson step (dyson.cpp).  H and S: [ns, nk, nso, nso]. */
+int gb200_dyson_set_hamiltonian(gb200_context* ctx, const double* H, const double* S);
+/* find_mu (dyson.cpp:101-174): bracket with step 0.5 then bisection to `tol`. */
+int gb200_dyson_find_mu(gb200_context* ctx, const double* Sigma1, const double* Sigma_tau, double mu0,
+                        double nel_target, double tol, double* mu_out, double* nel_out);
+/* compute_G (dyson.cpp:238-288): hermitizes Sigma1 and Sigma_tau in the
+ * caller's buffers as the reference does, writes G_tau [nts, ns, nk, nso, nso]. */
+int gb200_dyson_compute_G(gb200_context* ctx, double* Sigma1, double* Sigma_tau, double mu, double* G);
+/* Electron count n(mu) for given self-energies (compute_number_of_electrons, dyson.cpp:72-99). */
+int gb200_dyson_electrons(gb200_context* ctx, const double* Sigma1, const double* Sigma_tau, double mu,
+                          double* nel_out);
+/* (E_1b, E_HF, E_corr) of compute_energy (common_utils.cpp:5-55). */
+int gb200_energy(gb200_context* ctx, const double* G, const double* Sigma1, const double* Sigma_tau,
+                 double* e_out3);
+
+/* One self-consistency iteration on device buffers, the sequence mbpt.exe
+ * runs per iteration (mbpt_run.h:199-209, dyson.cpp:290-317):
+ *   Sigma1 = HF(dm(G)), Sigma_tau = GW(G), mu = find_mu (if nel_target > 0),
+ *   G <- compute_G, energies.
+ * G_dev is overwritten with the new Green's function. */
+int gb200_iteration_device(gb200_context* ctx, double* G_dev, double* Sigma1_dev, double* Sigma_dev,
+                           double madelung, double nel_target, double tol, double* mu_inout, double* e_out3,
+                           void* stream);
+
+/* Timing of the last gb200_gw_sigma* call by stage, milliseconds, CUDA events:
+ * out[0] P0, out[1] W solve and transforms, out[2] Sigma, out[3] total. */
+int gb200_last_timings(const gb200_context* ctx, float* out4);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GB200_H */

@@ -196,6 +196,12 @@ def eval_P0_tilde(G, v, k1, k1q, P0, ns, X2C=False):
             p0_contraction(Gb, Gq, v, P0[t], prefactor)
 
 
+def hermitian_from_lower(A):
+    """Hermitian matrix defined by the strict lower triangle and the real diagonal of A."""
+    L = np.tril(A, -1)
+    return L + np.conj(L.T) + np.diag(np.real(np.diag(A)))
+
+
 def symmetrize_P0(P0, nk):
     """P0/=nk, hermitize, P0(beta-tau)=P0(tau) (gw_cpu_kernel.cpp:217-225)."""
     nts = P0.shape[0]
@@ -207,15 +213,16 @@ def symmetrize_P0(P0, nk):
 def eval_P_tilde(P0, Tnt_b, Ttn_b):
     """tau -> i Omega, (I - P0)^-1 P0 per frequency, back to tau (gw_cpu_kernel.cpp:227-279).
 
-    The inverse uses a Hermitian solve against the identity (the reference uses
-    Eigen's LDLT, :245-249), then hermitizes the inverse (:250) and multiplies
-    (:251).
+    The reference inverts with Eigen's LDLT (:245-249), which reads only the
+    lower triangle and the real part of the diagonal of (I - P0(i Omega)); the
+    same Hermitian matrix is formed here (``hermitian_from_lower``) and
+    inverted, then the inverse is hermitized (:250) and multiplied (:251).
     """
     nts, NQ, _ = P0.shape
     Pw = (Tnt_b @ P0.reshape(nts, NQ * NQ)).reshape(-1, NQ, NQ)
     I = np.eye(NQ, dtype=np.complex128)
     for n in range(Pw.shape[0]):
-        temp = np.linalg.solve(I - Pw[n], I)
+        temp = np.linalg.solve(hermitian_from_lower(I - Pw[n]), I)
         temp = 0.5 * (temp + np.conj(temp.T))
         Pw[n] = temp @ Pw[n]
     return (Ttn_b @ Pw.reshape(Pw.shape[0], NQ * NQ)).reshape(nts, NQ, NQ)

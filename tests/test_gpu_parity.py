@@ -1,0 +1,128 @@
+"""GPU FP64 path against the CPU oracle, through the C ABI.
+
+Tolerance: 1e-10 relative to the largest element (the FP64 parity bar of the
+plain GPU path); the HF golden fixture is compared at the reference's own
+1e-10 absolute tolerance (test/tensor_test.h:41).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import gw_oracle as O
+from gb200 import lib, solvers
+from _systems import oracle_fock, oracle_sigma, rel, system
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+@pytest.fixture(scope="module")
+def ctx_small(gpu):
+    s = system("small")
+    c = solvers.make_context(s)
+    yield s, c
+    c.close()
+
+
+@pytest.mark.parametrize("name", ["small", "small_ns2", "odd_mesh", "c0"])
+def test_gw_sigma_parity(gpu, name):
+    s = system(name)
+    with solvers.make_context(s) as c:
+        sig = c.gw_sigma(s.G)
+    ref = oracle_sigma(name)
+    assert rel(sig, ref) < TOL
+
+
+@pytest.mark.parametrize("name", ["small", "small_ns2", "c0"])
+def test_hf_parity(gpu, name):
+    s = system(name)
+    with solvers.make_context(s) as c:
+        for mad in (0.0, 0.37):
+            dm = O.hf_density(s.G, s.ns)
+            F = c.hf_fock(dm, s.S, mad)
+            assert rel(F, oracle_fock(s, mad)) < TOL
+
+
+def test_hf_golden_through_gpu(gpu):
+    """The reference's HF fixture (k-point symmetry expanded on the host) through the GPU kernel."""
+    d = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "hf.npz")))
+    sym = O.RefSymmetry(d["bz2ibz"], d["ibz2bz"], d["tr_conj"], d["k_sym_transform_ao"], d["conj_pairs_list"],
+                        d["trans_pairs_list"], d["kpair_irre_list"], d["weight_ibz"])
+    ns, nk, nao, NQ = int(d["ns"]), int(d["nk"]), int(d["nao"]), int(d["NQ"])
+    dm_ibz = O.hf_density(d["G_beta"][None], ns)
+    dm = np.stack([np.stack([sym.value_AO(dm_ibz[s], k) for k in range(nk)]) for s in range(ns)])
+    S = np.stack([np.stack([sym.value_AO(d["S_ibz"][s], k) for k in range(nk)]) for s in range(ns)])
+    for s in range(ns):
+        for ik, k in enumerate(sym.ibz2bz):
+            S[s, k] = d["S_ibz"][s, ik]
+    Vh = np.stack([sym.integral(d["V_chunk"], k1, k2) for k1 in range(nk) for k2 in range(k1 + 1)])
+    with lib.Context(nk, nao, ns, NQ, 2, 2, 2, 100.0) as c:
+        c.set_integrals(Vh, lib.INTEGRALS_HF)
+        F = c.hf_fock(dm, S, float(d["madelung"]))
+    np.testing.assert_allclose(F[:, sym.ibz2bz], d["Sigma1"], rtol=0, atol=1e-10)
+
+
+def test_dyson_parity(gpu, ctx_small):
+    s, c = ctx_small
+    g = s.grid
+    sig = oracle_sigma("small")
+    F = oracle_fock(s)
+    mu = -0.3
+    G, S1h, Sth = c.compute_G(F, sig, mu)
+    Gref = O.compute_G(F, sig, s.F, s.S, mu, g.Tnt_f, g.Ttn_f, g.wsample_f)
+    assert rel(G, Gref) < TOL
+    assert rel(S1h, O.make_hermitian(F)) < 1e-14
+    ev = O.selfenergy_eigenspectra(F, sig, s.F, s.S, g.Tnt_f)
+    n_ref = O.number_of_electrons(mu, ev, g.Ttn_beta, g.wsample_f, s.ns, 1.0 / s.nk)
+    n_gpu = c.electrons(F, sig, mu)
+    assert abs(n_gpu - n_ref) < 1e-10 * abs(n_ref)
+    target = s.nel_from_G0()
+    nel_g, mu_g = c.find_mu(F, sig, 0.0, target, 1e-9)
+    nel_o, mu_o = O.find_mu(0.0, target, ev, g.Ttn_beta, g.wsample_f, s.ns, 1.0 / s.nk, 1e-9)
+    assert abs(mu_g - mu_o) < 1e-8
+    assert abs(nel_g - target) <= 1e-9 * target
+    e_gpu = c.energy(Gref, F, sig)
+    e_ref = O.compute_energy(Gref, F, sig, s.F, g.Tnt_f, g.Ttn_beta, 1.0 / s.nk)
+    np.testing.assert_allclose(e_gpu, e_ref, rtol=1e-10, atol=1e-12)
+
+
+def test_solver_mirror_iteration(gpu, ctx_small):
+    """gw_solver / hf_solver / dyson in the order of one reference SC iteration."""
+    s, c = ctx_small
+    G = s.G.copy()
+    S1 = np.zeros(c.shape_F, dtype=np.complex128)
+    St = np.zeros(c.shape_G, dtype=np.complex128)
+    solvers.hf_solver(c, s.S, 0.0, s.ns).solve(G, S1, St)
+    solvers.gw_solver(c).solve(G, S1, St)
+    dy = solvers.dyson(c, nel=s.nel_from_G0())
+    dy.solve(G, S1, St)
+    assert np.isfinite(G).all()
+    assert dy.diff(G, S1, St) > 0
+
+
+def test_determinism(gpu, ctx_small):
+    s, c = ctx_small
+    a = c.gw_sigma(s.G)
+    b = c.gw_sigma(s.G)
+    assert np.array_equal(a, b)
+
+
+def test_sigma_hermitian_and_finite(gpu, ctx_small):
+    s, c = ctx_small
+    sig = c.gw_sigma(s.G)
+    assert np.isfinite(sig).all()
+    assert np.abs(sig - np.conj(np.swapaxes(sig, -1, -2))).max() < 1e-9 * np.abs(sig).max()
+
+
+def test_wrong_grid_rejected(gpu):
+    with pytest.raises(lib.mbpt_wrong_grid):
+        lib.Context(4, 6, 1, 20, 21, 20, 21, 20.0)
+
+
+def test_missing_setup_is_an_error(gpu):
+    s = system("small")
+    g = s.grid
+    with lib.Context(s.nk, s.nao, s.ns, s.NQ, g.nts, g.nw, g.nw_b, s.beta) as c:
+        with pytest.raises(lib.mbpt_kernel_error):
+            c.gw_sigma(s.G)

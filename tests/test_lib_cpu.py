@@ -1,0 +1,58 @@
+"""Host-side checks that need no GPU: the library loads, exports the C ABI,
+and the input validation / version logic behaves like the reference."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from gb200 import lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", fn)).read()
+            names |= set(re.findall(r"\b(gb200_[A-Za-z0-9_]+)\s*\(", txt))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    L = lib.load()
+    names = declared_symbols()
+    assert "gb200_gw_sigma" in names and "gb200_hf_fock" in names
+    for n in sorted(names):
+        assert hasattr(L, n), f"missing export {n}"
+    assert set(lib.EXPORTED) <= names
+
+
+def test_version_check_matches_reference_rules():
+    # CheckVersion (common_defs.h:191-212) against INPUT_VERSION 1.0.0
+    assert lib.check_integral_version("1.0.0")
+    assert lib.check_integral_version("1.1.0")
+    assert lib.check_integral_version("1.0.0b10")
+    with pytest.raises(lib.mbpt_outdated_input):
+        lib.check_integral_version("0.3.0")
+    with pytest.raises(ValueError):
+        lib.check_integral_version("garbage")
+
+
+def test_create_rejects_bad_dims_without_gpu():
+    # argument validation happens before any CUDA call
+    with pytest.raises(lib.mbpt_wrong_grid):
+        lib.Context(4, 6, 1, 20, 21, 20, 21, 20.0)
+    with pytest.raises(lib.mbpt_kernel_error):
+        lib.Context(4, 6, 3, 20, 20, 20, 21, 20.0)
+    with pytest.raises(lib.mbpt_kernel_error):
+        lib.Context(4, 6, 1, 20, 20, 20, 21, 20.0, nso=12)  # X2C not on the GPU path
+
+
+def test_null_context_is_an_error():
+    L = lib.load()
+    assert L.gb200_gw_sigma(None, None, None) == lib.ERR_INVALID
+    t = (ctypes.c_float * 4)()
+    assert L.gb200_last_timings(None, t) == lib.ERR_INVALID

@@ -218,6 +218,13 @@ int gb200_set_precision(gb200_context* ctx, int mode, int slices) {
   });
 }
 
+int gb200_set_split_engine(gb200_context* ctx, int engine) {
+  return guarded(ctx, [&](Context& c) {
+    require(engine == 0 || engine == 1, GB200_ERR_INVALID, "set_split_engine: engine must be 0 or 1");
+    c.split_core = engine;
+  });
+}
+
 int gb200_gw_sigma(gb200_context* ctx, const double* G, double* Sigma) {
   return guarded(ctx, [&](Context& c) {
     require(G && Sigma, GB200_ERR_INVALID, "gw_sigma: null pointer");

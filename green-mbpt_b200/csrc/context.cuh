@@ -57,6 +57,8 @@ enum ScratchSlot {
   SL_IO_S1, SL_IO_H, SL_DM, SL_PINV, SL_SPLIT0, SL_COUNT
 };
 
+struct SplitEngine;
+
 struct Context {
   gb200_dims d{};
   int device = 0;
@@ -64,6 +66,8 @@ struct Context {
   std::string last_error;
   int prec_mode = GB200_PREC_FP64;
   int slices = 4;
+  int split_core = 0;             // 0: tcgen05 tensor cores, 1: CUDA-core validation core
+  SplitEngine* split = nullptr;
 
   bool have_kq = false, have_grid = false, have_V = false, have_Vhf = false, have_H = false;
   std::vector<int32_t> kplus, kminus;  // [nk * nk]

@@ -258,6 +258,10 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
     t_p0 += a_ms; t_w += b_ms; t_sig += c_ms;
   }
   scale_inplace(Sigma, c.g_elems(), 1.0 / nk, st);  // gw_cpu_kernel.cpp:55
+  if (se) {
+    int e = split_check_error(c, st);
+    require(e == 0, GB200_ERR_CUDA, "split contraction: tensor-core pipeline wait timed out (code " + std::to_string(e) + ")");
+  }
   GB_CUDA(cudaEventRecord(c.ev[4], st));
   GB_CUDA(cudaEventSynchronize(c.ev[4]));
   float tot = 0;

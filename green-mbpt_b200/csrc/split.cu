@@ -1,16 +1,709 @@
-// Split-precision contractions (filled in by the Ozaki INT8 engine).
+// Split-precision complex contractions: Ozaki slicing into INT8, exact INT32
+// products on the 5th-generation tensor cores (tcgen05, kind::i8), FP64
+// recombination.
+//
+// Number format.  Every complex row of the left operand (and every complex
+// column of the right one) gets a power-of-two exponent e with max|Re|,|Im| <
+// 2^e over the contraction range.  Each real part is cut into S signed 7-bit
+// slices by truncation, a = 2^(e-7) (q_0 + q_1 2^-7 + ... + q_{S-1} 2^-7(S-1)) + r,
+// |q_s| <= 127, which is exact in FP64 at every step.  Products of slices s and
+// t share the weight 2^-7(s+t); all pairs with s + t = d accumulate into one
+// INT32 accumulator "diagonal" d (pairs with s + t >= S are dropped, the usual
+// triangular Ozaki truncation).  The host splits the contraction so that no
+// diagonal can overflow INT32.
+//
+// Complex arithmetic.  A complex product becomes one real product through the
+// embedding  [Re A  -Im A; Im A  Re A] x [Re B; Im B]: the left operand is stored
+// with two interleaved real rows per complex row (2m: re,-im; 2m+1: im,re,
+// interleaved along K), the right operand as (re, im) pairs along K.  Real row
+// 2m of the result is Re C, row 2m+1 is Im C.
+//
+// Tensor-core kernel.  One CTA computes 128 real rows x BN complex columns for
+// all S diagonals (S * BN <= 512 TMEM columns).  Warp 0 streams 64-byte K blocks
+// of every slice plane with TMA (64-byte swizzle) through a multi-stage mbarrier
+// ring, warp 1 issues the tcgen05.mma instructions from one thread, and warps
+// 2-5 read the accumulators from TMEM (tcgen05.ld) and recombine in FP64.  Every
+// wait is bounded; on timeout the kernel records an error and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
 #include "split.cuh"
 
 namespace gb200 {
 
-struct SplitEngine {};
+namespace {
 
-SplitEngine* split_engine(Context&) { throw Error(GB200_ERR_INVALID, "split precision not built"); }
-void split_prepare_integrals(Context&, SplitEngine&, cudaStream_t) {}
-void split_gemm(Context&, SplitEngine&, const ZGemm&, cudaStream_t) {
-  throw Error(GB200_ERR_INVALID, "split precision not built");
+constexpr int KBLK = 64;          // bytes of K per pipeline stage (one 64B swizzle atom)
+constexpr int TILE_M = 128;       // real rows per CTA (64 complex rows)
+constexpr int SMEM_BUDGET = 200 * 1024;
+constexpr int NWARPS = 6;
+constexpr long long WAIT_LIMIT = 4000000000LL;  // clock64 cycles (~2 s)
+
+enum SplitErr { SERR_NONE = 0, SERR_TIMEOUT_PRODUCER = 1, SERR_TIMEOUT_MMA = 2, SERR_TIMEOUT_EPILOGUE = 3 };
+
+// ----------------------------------------------------------------------------
+// PTX wrappers
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: returns false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, volatile int* abort_flag) {
+  long long t0 = clock64();
+  while (!mbar_try_wait(bar, phase)) {
+    if (*abort_flag) return false;
+    if (clock64() - t0 > WAIT_LIMIT) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(smem_dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)), "r"(ncols));
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
+}
+
+__device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Shared-memory matrix descriptor: K-major operand, 64-byte swizzle, rows of
+// 64 bytes, 8-row groups 512 bytes apart (SBO), layout version 1 (sm_100).
+__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;            // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;   // stride byte offset
+  d |= (uint64_t)1 << 46;            // descriptor version
+  d |= (uint64_t)4 << 61;            // SWIZZLE_64B
+  return d;
+}
+
+// Instruction descriptor: S32 accumulate, signed 8-bit A and B, both K-major, M=128, N=bn.
+__host__ __device__ constexpr uint32_t idesc_i8(int bn) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(bn >> 3) << 17) | ((uint32_t)(TILE_M >> 4) << 24);
+}
+
+// ----------------------------------------------------------------------------
+// parameters
+// ----------------------------------------------------------------------------
+struct OperandSlices {
+  int64_t nrb = 1;             // reduced batch count
+  int dep[3] = {0, 0, 0};      // which batch components the operand depends on
+  int64_t R = 0;               // complex rows (A: M, B: N)
+  int64_t rows_pad = 0;        // real rows per plane
+  int64_t kpad = 0;            // bytes per row
+  int64_t e_ld = 0;            // exponents per reduced batch
+  int8_t* planes = nullptr;    // [nrb][S][rows_pad][kpad]
+  int32_t* expo = nullptr;     // [nrb][e_ld]
+};
+
+struct GemmParams {
+  int S;
+  int BN;
+  int nkb;
+  int ntiles_n;
+  int64_t M, N;
+  int64_t nb0, nb1, nb2;
+  int depA[3], depB[3];
+  int64_t rowsA_pad, rowsB_pad;
+  const int32_t* eA;
+  const int32_t* eB;
+  int64_t eA_ld, eB_ld;
+  ZResult C;
+  cplx alpha, beta;
+  int* err;
+};
+
+__device__ __forceinline__ int64_t reduced_batch(const int dep[3], int64_t b0, int64_t b1, int64_t b2, int64_t n1,
+                                                 int64_t n2) {
+  int64_t rb = 0;
+  if (dep[0]) rb = b0;
+  if (dep[1]) rb = rb * n1 + b1;
+  if (dep[2]) rb = rb * n2 + b2;
+  return rb;
+}
+
+// ----------------------------------------------------------------------------
+// slicing
+// ----------------------------------------------------------------------------
+struct SliceJob {
+  const cplx* ptr;
+  IdxMap rmap, kmap;
+  BatchMap bat;
+  bool conj;
+  int64_t R, K, k0;            // rows, K range [k0, k0 + K)
+  int64_t n0, n1, n2;          // batch sizes of the GEMM
+  int dep[3];
+  int embed;                   // 1: left operand (doubled rows), 0: right operand
+  int S;
+  int64_t rows_pad, kpad, e_ld;
+  int8_t* out;
+  int32_t* expo;
+  bool r_fast;                 // consecutive threads walk rows (else K) when reading
+};
+
+constexpr int SL_ROWS = 32, SL_K = 32, SL_NT = 256;
+
+__device__ __forceinline__ void enumerate_batch(const SliceJob& j, int64_t rb, int64_t& b0, int64_t& b1, int64_t& b2) {
+  // inverse of reduced_batch with non-dependent components set to 0
+  b0 = b1 = b2 = 0;
+  int64_t r = rb;
+  if (j.dep[2]) { b2 = r % j.n2; r /= j.n2; }
+  if (j.dep[1]) { b1 = r % j.n1; r /= j.n1; }
+  if (j.dep[0]) { b0 = r; }
+}
+
+// One block handles SL_ROWS complex rows of one reduced batch: pass 1 finds the
+// per-row exponent, pass 2 writes the slice planes.
+__global__ void __launch_bounds__(SL_NT) slice_kernel(SliceJob j) {
+  __shared__ cplx tile[SL_ROWS][SL_K + 1];
+  __shared__ double rmax[SL_ROWS];
+  __shared__ int rexp[SL_ROWS];
+  __shared__ int64_t roff[SL_ROWS];
+  const int64_t rb = blockIdx.y;
+  const int64_t r0 = (int64_t)blockIdx.x * SL_ROWS;
+  int64_t b0, b1, b2;
+  enumerate_batch(j, rb, b0, b1, b2);
+  const cplx* base = j.ptr + j.bat(b0, b1, b2);
+  const int tid = threadIdx.x;
+  if (tid < SL_ROWS) {
+    int64_t r = r0 + tid;
+    roff[tid] = r < j.R ? j.rmap(r) : 0;
+    rmax[tid] = 0.0;
+  }
+  __syncthreads();
+  auto load_tile = [&](int64_t kc) {
+    for (int e = tid; e < SL_ROWS * SL_K; e += SL_NT) {
+      int rl, kl;
+      if (j.r_fast) { rl = e % SL_ROWS; kl = e / SL_ROWS; } else { kl = e % SL_K; rl = e / SL_K; }
+      int64_t r = r0 + rl, k = kc + kl;
+      cplx v = cmk(0.0, 0.0);
+      if (r < j.R && k < j.K) {
+        v = base[roff[rl] + j.kmap(j.k0 + k)];
+        if (j.conj) v.y = -v.y;
+      }
+      tile[rl][kl] = v;
+    }
+  };
+  // pass 1: row maxima
+  for (int64_t kc = 0; kc < j.K; kc += SL_K) {
+    load_tile(kc);
+    __syncthreads();
+    for (int e = tid; e < SL_ROWS * SL_K; e += SL_NT) {
+      int rl = e / SL_K, kl = e % SL_K;
+      cplx v = tile[rl][kl];
+      double m = fmax(fabs(v.x), fabs(v.y));
+      // warp lanes of one row: SL_K == 32 consecutive e share rl
+      for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if ((tid & 31) == 0) rmax[rl] = fmax(rmax[rl], m);
+    }
+    __syncthreads();
+  }
+  if (tid < SL_ROWS) {
+    int e = 0;
+    if (rmax[tid] > 0.0) frexp(rmax[tid], &e);  // rmax < 2^e
+    rexp[tid] = e;
+    int64_t r = r0 + tid;
+    if (r < j.R) j.expo[rb * j.e_ld + r] = e;
+  }
+  __syncthreads();
+  // pass 2: slices
+  const int64_t plane = j.rows_pad * j.kpad;
+  int8_t* outb = j.out + rb * (int64_t)j.S * plane;
+  for (int64_t kc = 0; kc < j.K; kc += SL_K) {
+    load_tile(kc);
+    __syncthreads();
+    for (int e = tid; e < SL_ROWS * SL_K; e += SL_NT) {
+      int rl = e / SL_K, kl = e % SL_K;
+      int64_t r = r0 + rl, k = kc + kl;
+      if (r >= j.R || k >= j.K) continue;
+      cplx v = tile[rl][kl];
+      const int ex = rexp[rl];
+      double xr = ldexp(v.x, 7 - ex), xi = ldexp(v.y, 7 - ex);
+      for (int s = 0; s < j.S; ++s) {
+        double qr = trunc(xr), qi = trunc(xi);
+        int8_t ar = (int8_t)(int)qr, ai = (int8_t)(int)qi;
+        xr = (xr - qr) * 128.0;
+        xi = (xi - qi) * 128.0;
+        int8_t* p = outb + (int64_t)s * plane;
+        if (j.embed) {
+          int64_t row0 = 2 * r;
+          char2 w0 = make_char2(ar, (int8_t)(-ai));
+          char2 w1 = make_char2(ai, ar);
+          *reinterpret_cast<char2*>(p + row0 * j.kpad + 2 * k) = w0;
+          *reinterpret_cast<char2*>(p + (row0 + 1) * j.kpad + 2 * k) = w1;
+        } else {
+          *reinterpret_cast<char2*>(p + r * j.kpad + 2 * k) = make_char2(ar, ai);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ----------------------------------------------------------------------------
+// recombination epilogue (shared by both cores)
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ void store_result(const GemmParams& p, int64_t b0, int64_t b1, int64_t b2, int64_t m, int64_t n,
+                                             double re, double im, int ea, int eb) {
+  cplx* Cb = p.C.ptr + p.C.bat(b0, b1, b2);
+  cplx* dst = Cb + p.C.row(m) + p.C.col(n);
+  cplx v = cmk(ldexp(re, ea + eb), ldexp(im, ea + eb));
+  v = cmul(p.alpha, v);
+  if (p.beta.x != 0.0 || p.beta.y != 0.0) v = cadd(v, cmul(p.beta, *dst));
+  *dst = v;
+}
+
+// ----------------------------------------------------------------------------
+// tcgen05 core
+// ----------------------------------------------------------------------------
+struct SmemLayout {
+  int stage_bytes, a_plane_bytes, b_plane_bytes, stages;
+};
+
+__host__ __device__ inline SmemLayout smem_layout(int S, int BN) {
+  SmemLayout L;
+  L.a_plane_bytes = TILE_M * KBLK;
+  L.b_plane_bytes = BN * KBLK;
+  L.stage_bytes = S * (L.a_plane_bytes + L.b_plane_bytes);
+  L.stages = (SMEM_BUDGET - 2048) / L.stage_bytes;
+  if (L.stages > 6) L.stages = 6;
+  return L;
+}
+
+__global__ void __launch_bounds__(NWARPS * 32, 1)
+    split_gemm_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, GemmParams p) {
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  // 1024-byte aligned base for the swizzled tiles
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const SmemLayout L = smem_layout(p.S, p.BN);
+  uint8_t* tiles = smem;
+  uint64_t* full_bar = reinterpret_cast<uint64_t*>(tiles + (size_t)L.stages * L.stage_bytes);
+  uint64_t* empty_bar = full_bar + L.stages;
+  uint64_t* accum_bar = empty_bar + L.stages;
+  uint8_t* misc = reinterpret_cast<uint8_t*>(accum_bar + 1);
+  uint32_t* tmem_base_slot = reinterpret_cast<uint32_t*>(misc);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(misc + 4);
+  int32_t* sh_eA = reinterpret_cast<int32_t*>(misc + 8);
+  int32_t* sh_eB = sh_eA + TILE_M / 2;
+
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int64_t bz = blockIdx.z;
+  const int64_t b2 = bz % p.nb2, b1 = (bz / p.nb2) % p.nb1, b0 = bz / (p.nb2 * p.nb1);
+  const int64_t rbA = reduced_batch(p.depA, b0, b1, b2, p.nb1, p.nb2);
+  const int64_t rbB = reduced_batch(p.depB, b0, b1, b2, p.nb1, p.nb2);
+  const int64_t mrow0 = (int64_t)blockIdx.y * TILE_M;  // real rows
+  const int64_t ncol0 = (int64_t)blockIdx.x * p.BN;    // complex columns
+  const int S = p.S;
+  const uint32_t ncols_alloc = (S * p.BN <= 32) ? 32 : (S * p.BN <= 64) ? 64 : (S * p.BN <= 128) ? 128 : (S * p.BN <= 256) ? 256 : 512;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < L.stages; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(accum_bar, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(tmem_base_slot, ncols_alloc);
+  // exponents of this tile
+  for (int i = threadIdx.x; i < TILE_M / 2 + p.BN; i += blockDim.x) {
+    if (i < TILE_M / 2) {
+      int64_t m = mrow0 / 2 + i;
+      sh_eA[i] = m < p.M ? p.eA[rbA * p.eA_ld + m] : 0;
+    } else {
+      int64_t n = ncol0 + (i - TILE_M / 2);
+      sh_eB[i - TILE_M / 2] = n < p.N ? p.eB[rbB * p.eB_ld + n] : 0;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_base_slot;
+
+  int issued = 0;  // producer: number of stages issued
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int kb = 0; kb < p.nkb; ++kb) {
+        const int st = kb % L.stages;
+        const uint32_t ph = (kb / L.stages) & 1;
+        if (kb >= L.stages) {
+          if (!mbar_wait(&empty_bar[st], ph ^ 1, abort_flag)) {
+            atomicExch(p.err, SERR_TIMEOUT_PRODUCER);
+            *abort_flag = 1;
+            break;
+          }
+        }
+        uint8_t* sbase = tiles + (size_t)st * L.stage_bytes;
+        mbar_expect_tx(&full_bar[st], (uint32_t)L.stage_bytes);
+        for (int s = 0; s < S; ++s) {
+          const int ya = (int)((rbA * S + s) * p.rowsA_pad + mrow0);
+          tma_load_2d(sbase + s * L.a_plane_bytes, &mapA, kb * KBLK, ya, &full_bar[st]);
+        }
+        uint8_t* bbase = sbase + S * L.a_plane_bytes;
+        for (int t = 0; t < S; ++t) {
+          const int yb = (int)((rbB * S + t) * p.rowsB_pad + ncol0);
+          tma_load_2d(bbase + t * L.b_plane_bytes, &mapB, kb * KBLK, yb, &full_bar[st]);
+        }
+        issued = kb + 1;
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = idesc_i8(p.BN);
+      bool ok = true;
+      for (int kb = 0; kb < p.nkb; ++kb) {
+        const int st = kb % L.stages;
+        const uint32_t ph = (kb / L.stages) & 1;
+        if (!mbar_wait(&full_bar[st], ph, abort_flag)) {
+          atomicExch(p.err, SERR_TIMEOUT_MMA);
+          *abort_flag = 1;
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        uint8_t* sbase = tiles + (size_t)st * L.stage_bytes;
+        uint8_t* bbase = sbase + S * L.a_plane_bytes;
+        for (int s = 0; s < S; ++s) {
+          const uint64_t ad = smem_desc_sw64(smem_u32(sbase + s * L.a_plane_bytes));
+          for (int t = 0; s + t < S; ++t) {
+            const uint64_t bd = smem_desc_sw64(smem_u32(bbase + t * L.b_plane_bytes));
+            const uint32_t dt = tmem_base + (uint32_t)((s + t) * p.BN);
+#pragma unroll
+            for (int kk = 0; kk < KBLK / 32; ++kk) {
+              // +32 bytes along K inside the swizzle atom = +2 in the encoded address
+              umma_i8(dt, ad + 2 * kk, bd + 2 * kk, idesc, (kb > 0 || kk > 0 || s > 0) ? 1u : 0u);
+            }
+          }
+        }
+        umma_commit(&empty_bar[st]);
+      }
+      if (ok) umma_commit(accum_bar);
+    }
+  } else {
+    // epilogue warps 2..5: TMEM sub-partition = warp % 4
+    const int sp = warp % 4;
+    const int row = sp * 32 + lane;  // real row inside the tile
+    bool ok = true;
+    if (lane == 0) {
+      ok = mbar_wait(accum_bar, 0, abort_flag);
+    }
+    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+    if (!ok) {
+      if (lane == 0) {
+        atomicExch(p.err, SERR_TIMEOUT_EPILOGUE);
+        *abort_flag = 1;
+      }
+    } else {
+      tc_fence_after();
+      const int64_t mreal = mrow0 + row;
+      const int64_t m = mreal / 2;
+      const int r = (int)(mreal & 1);
+      const int ea = sh_eA[row / 2];
+      for (int c0 = 0; c0 < p.BN; c0 += 16) {
+        double v[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = 0.0;
+        for (int d = 0; d < S; ++d) {
+          int32_t q[16];
+          tmem_ld16(tmem_base + ((uint32_t)(sp * 32) << 16) + (uint32_t)(d * p.BN + c0), q);
+          tmem_wait_ld();
+          const double w = ldexp(1.0, -7 * (d + 2));
+#pragma unroll
+          for (int j = 0; j < 16; ++j) v[j] = fma((double)q[j], w, v[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          double other = __shfl_xor_sync(0xffffffffu, v[j], 1);
+          const int64_t n = ncol0 + c0 + j;
+          if (r == 0 && m < p.M && n < p.N) store_result(p, b0, b1, b2, m, n, v[j], other, ea, sh_eB[c0 + j]);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  // after an abort, let in-flight TMA loads land before the shared memory is released
+  if (warp == 0 && lane == 0 && *abort_flag) {
+    for (int kb = 0; kb < issued; ++kb) {
+      long long t0 = clock64();
+      while (!mbar_try_wait(&full_bar[kb % L.stages], (kb / L.stages) & 1)) {
+        if (clock64() - t0 > WAIT_LIMIT) break;
+      }
+    }
+  }
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, ncols_alloc);
+  }
+}
+
+// ----------------------------------------------------------------------------
+// CUDA-core validation core: the same diagonal INT32 sums from the same planes.
+// ----------------------------------------------------------------------------
+__global__ void split_gemm_ref_kernel(const int8_t* Ap, const int8_t* Bp, int64_t kpad, GemmParams p) {
+  const int64_t bz = blockIdx.z;
+  const int64_t b2 = bz % p.nb2, b1 = (bz / p.nb2) % p.nb1, b0 = bz / (p.nb2 * p.nb1);
+  const int64_t rbA = reduced_batch(p.depA, b0, b1, b2, p.nb1, p.nb2);
+  const int64_t rbB = reduced_batch(p.depB, b0, b1, b2, p.nb1, p.nb2);
+  const int64_t m = (int64_t)blockIdx.y * 16 + threadIdx.y;
+  const int64_t n = (int64_t)blockIdx.x * 16 + threadIdx.x;
+  if (m >= p.M || n >= p.N) return;
+  const int S = p.S;
+  double re = 0.0, im = 0.0;
+  for (int d = 0; d < S; ++d) {
+    int32_t accr = 0, acci = 0;
+    for (int s = 0; s <= d; ++s) {
+      const int t = d - s;
+      const int8_t* a0 = Ap + ((rbA * S + s) * p.rowsA_pad + 2 * m) * kpad;
+      const int8_t* a1 = a0 + kpad;
+      const int8_t* bb = Bp + ((rbB * S + t) * p.rowsB_pad + n) * kpad;
+      for (int64_t k = 0; k < kpad; ++k) {
+        accr += (int32_t)a0[k] * (int32_t)bb[k];
+        acci += (int32_t)a1[k] * (int32_t)bb[k];
+      }
+    }
+    const double w = ldexp(1.0, -7 * (d + 2));
+    re = fma((double)accr, w, re);
+    im = fma((double)acci, w, im);
+  }
+  store_result(p, b0, b1, b2, m, n, re, im, p.eA[rbA * p.eA_ld + m], p.eB[rbB * p.eB_ld + n]);
+}
+
+// ----------------------------------------------------------------------------
+// host side
+// ----------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  });
+  require(fn != nullptr, GB200_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  return fn;
+}
+
+CUtensorMap make_map(const int8_t* base, int64_t kpad, int64_t rows_total, int box_rows) {
+  CUtensorMap m;
+  std::memset(&m, 0, sizeof(m));
+  cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows_total};
+  cuuint64_t strides[1] = {(cuuint64_t)kpad};
+  cuuint32_t box[2] = {(cuuint32_t)KBLK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  require((reinterpret_cast<uintptr_t>(base) & 15) == 0 && kpad % 16 == 0, GB200_ERR_INVALID, "TMA alignment");
+  CUresult r = get_encode()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(base), dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  require(r == CUDA_SUCCESS, GB200_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+  return m;
+}
+
+inline int64_t rup(int64_t a, int64_t b) { return (a + b - 1) / b * b; }
+
+void deps_of(const ZOperand& o, int dep[3]) {
+  dep[0] = (o.bat.tab0 != nullptr || o.bat.s0 != 0) ? 1 : 0;
+  dep[1] = o.bat.s1 != 0 ? 1 : 0;
+  dep[2] = o.bat.s2 != 0 ? 1 : 0;
+}
+
+int64_t nrb_of(const int dep[3], const ZGemm& g) {
+  int64_t n = 1;
+  if (dep[0]) n *= g.nb0;
+  if (dep[1]) n *= g.nb1;
+  if (dep[2]) n *= g.nb2;
+  return n;
+}
+
+}  // namespace
+
+struct SplitEngine {
+  int core = 0;  // 0: tcgen05, 1: CUDA-core validation core
+  DevArray<int8_t> planesA, planesB;
+  DevArray<int32_t> expA, expB;
+  DevArray<int> err;
+  bool attr_set = false;
+};
+
+SplitEngine* split_engine(Context& c) {
+  if (!c.split) c.split = new SplitEngine();
+  c.split->core = c.split_core;
+  return c.split;
+}
+
+void split_prepare_integrals(Context&, SplitEngine&, cudaStream_t) {}
+
 void split_invalidate(Context&) {}
-void split_release(Context&) {}
+
+void split_release(Context& c) {
+  delete c.split;
+  c.split = nullptr;
+}
+
+void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st) {
+  if (g0.M <= 0 || g0.N <= 0) return;
+  validate(g0);
+  const int S = c.slices;
+  require(S >= 2 && S <= 8, GB200_ERR_INVALID, "split: slices out of range");
+  require(g0.K > 0, GB200_ERR_INVALID, "split: empty contraction");
+  const int BN = (S <= 4) ? 128 : 64;
+  const SmemLayout L = smem_layout(S, BN);
+  require(L.stages >= 2, GB200_ERR_INVALID, "split: shared memory too small");
+  // largest K chunk for which no INT32 diagonal can overflow: S * 2K * 127^2 < 2^31
+  int64_t kmax = (int64_t)(2147483647.0 / (2.0 * 127.0 * 127.0 * S));
+  kmax = kmax / 32 * 32;
+  int depA[3], depB[3];
+  deps_of(g0.A, depA);
+  deps_of(g0.B, depB);
+  const int64_t nrbA = nrb_of(depA, g0), nrbB = nrb_of(depB, g0);
+  const int64_t rowsA_pad = rup(2 * g0.M, TILE_M);
+  const int64_t rowsB_pad = rup(g0.N, BN);
+  if (!se.err.p) {
+    se.err.alloc(1);
+    GB_CUDA(cudaMemsetAsync(se.err.p, 0, sizeof(int), st));
+  }
+  for (int64_t k0 = 0; k0 < g0.K; k0 += kmax) {
+    const int64_t Kc = std::min(kmax, g0.K - k0);
+    const int64_t kpad = rup(2 * Kc, KBLK);
+    se.planesA.alloc((size_t)(nrbA * S * rowsA_pad * kpad));
+    se.planesB.alloc((size_t)(nrbB * S * rowsB_pad * kpad));
+    se.expA.alloc((size_t)(nrbA * rowsA_pad / 2));
+    se.expB.alloc((size_t)(nrbB * rowsB_pad));
+    // padding rows and K tails must read as zero
+    GB_CUDA(cudaMemsetAsync(se.planesA.p, 0, (size_t)(nrbA * S * rowsA_pad * kpad), st));
+    GB_CUDA(cudaMemsetAsync(se.planesB.p, 0, (size_t)(nrbB * S * rowsB_pad * kpad), st));
+    {
+      SliceJob j{};
+      j.ptr = g0.A.ptr; j.rmap = g0.A.row; j.kmap = g0.A.col; j.bat = g0.A.bat; j.conj = g0.A.conj;
+      j.R = g0.M; j.K = Kc; j.k0 = k0; j.n0 = g0.nb0; j.n1 = g0.nb1; j.n2 = g0.nb2;
+      std::copy(depA, depA + 3, j.dep);
+      j.embed = 1; j.S = S; j.rows_pad = rowsA_pad; j.kpad = kpad; j.e_ld = rowsA_pad / 2;
+      j.out = se.planesA.p; j.expo = se.expA.p;
+      j.r_fast = std::abs(g0.A.row.s_in) < std::abs(g0.A.col.s_in);
+      dim3 grid((unsigned)((g0.M + SL_ROWS - 1) / SL_ROWS), (unsigned)nrbA);
+      require(nrbA < 65536, GB200_ERR_INVALID, "split: too many batches");
+      slice_kernel<<<grid, SL_NT, 0, st>>>(j);
+      GB_CHECK_LAUNCH();
+    }
+    {
+      SliceJob j{};
+      // right operand sliced per column: rows of the job are the N columns, K runs along B's rows
+      j.ptr = g0.B.ptr; j.rmap = g0.B.col; j.kmap = g0.B.row; j.bat = g0.B.bat; j.conj = g0.B.conj;
+      j.R = g0.N; j.K = Kc; j.k0 = k0; j.n0 = g0.nb0; j.n1 = g0.nb1; j.n2 = g0.nb2;
+      std::copy(depB, depB + 3, j.dep);
+      j.embed = 0; j.S = S; j.rows_pad = rowsB_pad; j.kpad = kpad; j.e_ld = rowsB_pad;
+      j.out = se.planesB.p; j.expo = se.expB.p;
+      j.r_fast = std::abs(g0.B.col.s_in) < std::abs(g0.B.row.s_in);
+      dim3 grid((unsigned)((g0.N + SL_ROWS - 1) / SL_ROWS), (unsigned)nrbB);
+      require(nrbB < 65536, GB200_ERR_INVALID, "split: too many batches");
+      slice_kernel<<<grid, SL_NT, 0, st>>>(j);
+      GB_CHECK_LAUNCH();
+    }
+    GemmParams p{};
+    p.S = S; p.BN = BN; p.nkb = (int)(kpad / KBLK);
+    p.M = g0.M; p.N = g0.N; p.nb0 = g0.nb0; p.nb1 = g0.nb1; p.nb2 = g0.nb2;
+    std::copy(depA, depA + 3, p.depA);
+    std::copy(depB, depB + 3, p.depB);
+    p.rowsA_pad = rowsA_pad; p.rowsB_pad = rowsB_pad;
+    p.eA = se.expA.p; p.eB = se.expB.p; p.eA_ld = rowsA_pad / 2; p.eB_ld = rowsB_pad;
+    p.C = g0.C; p.alpha = g0.alpha; p.beta = (k0 == 0) ? g0.beta : cmk(1.0, 0.0);
+    p.err = se.err.p;
+    const int64_t nbatch = g0.nb0 * g0.nb1 * g0.nb2;
+    require(nbatch < 65536, GB200_ERR_INVALID, "split: too many batches for one launch");
+    if (se.core == 1) {
+      dim3 grid((unsigned)((g0.N + 15) / 16), (unsigned)((g0.M + 15) / 16), (unsigned)nbatch);
+      split_gemm_ref_kernel<<<grid, dim3(16, 16), 0, st>>>(se.planesA.p, se.planesB.p, kpad, p);
+      GB_CHECK_LAUNCH();
+    } else {
+      const int64_t rowsA_total = nrbA * S * rowsA_pad;
+      const int64_t rowsB_total = nrbB * S * rowsB_pad;
+      require(rowsA_total < (1LL << 31) && rowsB_total < (1LL << 31), GB200_ERR_INVALID, "split: operand too large for TMA");
+      CUtensorMap mA = make_map(se.planesA.p, kpad, rowsA_total, TILE_M);
+      CUtensorMap mB = make_map(se.planesB.p, kpad, rowsB_total, BN);
+      const size_t smem = (size_t)L.stages * L.stage_bytes + 1024 /*align*/ + 1024 /*barriers, exponents*/;
+      if (!se.attr_set) {
+        GB_CUDA(cudaFuncSetAttribute(split_gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        se.attr_set = true;
+      }
+      dim3 grid((unsigned)(rowsB_pad / BN), (unsigned)(rowsA_pad / TILE_M), (unsigned)nbatch);
+      split_gemm_tc_kernel<<<grid, NWARPS * 32, smem, st>>>(mA, mB, p);
+      GB_CHECK_LAUNCH();
+    }
+  }
+}
+
+int split_check_error(Context& c, cudaStream_t st) {
+  if (!c.split || !c.split->err.p) return 0;
+  int h = 0;
+  GB_CUDA(cudaMemcpyAsync(&h, c.split->err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  GB_CUDA(cudaStreamSynchronize(st));
+  if (h) GB_CUDA(cudaMemsetAsync(c.split->err.p, 0, sizeof(int), st));
+  return h;
+}
 
 }  // namespace gb200

@@ -17,5 +17,7 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g, cudaStream_t st);
 // Drop cached slices (integrals or precision changed).
 void split_invalidate(Context& c);
 void split_release(Context& c);
+// Non-zero if a split kernel hit a bounded-wait timeout since the last check (flag is cleared).
+int split_check_error(Context& c, cudaStream_t st);
 
 }  // namespace gb200

@@ -58,7 +58,7 @@ EXPORTED = [
     "gb200_set_kq_maps", "gb200_set_grid", "gb200_set_integrals", "gb200_set_precision", "gb200_gw_sigma",
     "gb200_gw_sigma_device", "gb200_hf_fock", "gb200_hf_fock_device", "gb200_dyson_set_hamiltonian",
     "gb200_dyson_find_mu", "gb200_dyson_compute_G", "gb200_dyson_electrons", "gb200_energy",
-    "gb200_iteration_device", "gb200_last_timings",
+    "gb200_iteration_device", "gb200_last_timings", "gb200_set_split_engine",
 ]
 
 
@@ -103,6 +103,7 @@ def load(path: str | None = None):
     L.gb200_energy.argtypes = [vp, vp, vp, vp, dp]
     L.gb200_iteration_device.argtypes = [vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, dp, dp, vp]
     L.gb200_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    L.gb200_set_split_engine.argtypes = [vp, ip]
     _lib = L
     return L
 
@@ -181,6 +182,10 @@ class Context:
 
     def set_precision(self, mode=PREC_FP64, slices=4):
         self._check(self._L.gb200_set_precision(self._h, mode, slices))
+
+    def set_split_engine(self, engine: int):
+        """0: tcgen05 tensor cores, 1: CUDA-core validation engine (bit-identical INT32 sums)."""
+        self._check(self._L.gb200_set_split_engine(self._h, engine))
 
     def set_hamiltonian(self, H, S):
         self._H, self._S = _c128(H), _c128(S)

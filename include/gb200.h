@@ -129,6 +129,12 @@ int gb200_iteration_device(gb200_context* ctx, double* G_dev, double* Sigma1_dev
                            double madelung, double nel_target, double tol, double* mu_inout, double* e_out3,
                            void* stream);
 
+/* Select the engine that multiplies the INT8 slice planes of GB200_PREC_SPLIT:
+ * 0 = tcgen05 tensor cores (default), 1 = CUDA-core validation engine that
+ * forms the same INT32 diagonal sums from the same planes (results must agree
+ * bit for bit).  No counterpart in the reference (its kernels are FP64 only). */
+int gb200_set_split_engine(gb200_context* ctx, int engine);
+
 /* Timing of the last gb200_gw_sigma* call by stage, milliseconds, CUDA events:
  * out[0] P0, out[1] W solve and transforms, out[2] Sigma, out[3] total. */
 int gb200_last_timings(const gb200_context* ctx, float* out4);

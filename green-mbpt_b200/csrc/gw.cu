@@ -148,14 +148,16 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
       const int64_t* tVp = c.tab_pair_plus.get() + (int64_t)q * nk + k0;
       const int64_t* tGp = c.tab_g_plus.get() + (int64_t)q * nk + k0;
       const int64_t blkT1 = (int64_t)nth * ns * pe;  // per kk in T1
-      // (a) T1[kk][t][s][(Q,p)][n] = sum_m V(k,k+q)[(Q,p)][m] G(t,s,k+q)[m][n]
+      // (a) T1[kk][t][s][(Q,p)][n] = sum_m V(k,k+q)[(Q,p)][m] G(t,s,k+q)[m][n]; the (t,s) pairs of
+      //     the first half of the grid are folded into the columns: one GEMM per k,
+      //     M = NQ*nao rows (Q,p), N = nth*ns*nao columns ((t,s),n), K = nao
       ZGemm a;
-      a.M = (int64_t)NQ * nao; a.N = nao; a.K = nao;
-      a.nb0 = kbk; a.nb1 = nth; a.nb2 = ns;
+      a.M = (int64_t)NQ * nao; a.N = (int64_t)nth * ns * nao; a.K = nao;
+      a.nb0 = kbk;
       a.A = dense(c.V.get(), nao); a.A.bat.tab0 = tVp;
-      a.B = dense(G, nao); a.B.bat.tab0 = tGp; a.B.bat.s1 = g_t; a.B.bat.s2 = g_s;
-      a.C.ptr = X1; a.C.row = lin(nao); a.C.col = lin(1);
-      a.C.bat.s0 = blkT1; a.C.bat.s1 = (int64_t)ns * pe; a.C.bat.s2 = pe;
+      a.B.ptr = G; a.B.row = lin(nao); a.B.col = two(nao, 1, g_s); a.B.bat.tab0 = tGp;
+      a.C.ptr = X1; a.C.row = lin(nao); a.C.col = two(nao, 1, pe);
+      a.C.bat.s0 = blkT1;
       // (b) Bt[t][kk][s][Q][r][n] = sum_p Gbar(nts-1-t, s, k)[r][p] T1[kk][t][s][Q][p][n]
       ZGemm b;
       b.M = nao; b.N = (int64_t)NQ * nao; b.K = nao;
@@ -217,14 +219,15 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
       const int64_t* tVm = c.tab_pair_minus.get() + (int64_t)q * nk + k0;
       const int64_t* tGm = c.tab_g_minus.get() + (int64_t)q * nk + k0;
       const int64_t blk = (int64_t)nts * ns * pe;  // per kk in Y1 / Y2
-      // (d) Y1[kk][t][s][(Q,i)][n] = sum_m V(k,k-q)[(Q,i)][m] G(t,s,k-q)[m][n]
+      // (d) Y1[kk][t][s][(Q,i)][n] = sum_m V(k,k-q)[(Q,i)][m] G(t,s,k-q)[m][n]; (t,s) folded into
+      //     the columns as in (a)
       ZGemm dd;
-      dd.M = (int64_t)NQ * nao; dd.N = nao; dd.K = nao;
-      dd.nb0 = kbk; dd.nb1 = nts; dd.nb2 = ns;
+      dd.M = (int64_t)NQ * nao; dd.N = (int64_t)nts * ns * nao; dd.K = nao;
+      dd.nb0 = kbk;
       dd.A = dense(c.V.get(), nao); dd.A.bat.tab0 = tVm;
-      dd.B = dense(G, nao); dd.B.bat.tab0 = tGm; dd.B.bat.s1 = g_t; dd.B.bat.s2 = g_s;
-      dd.C.ptr = X1; dd.C.row = lin(nao); dd.C.col = lin(1);
-      dd.C.bat.s0 = blk; dd.C.bat.s1 = (int64_t)ns * pe; dd.C.bat.s2 = pe;
+      dd.B.ptr = G; dd.B.row = lin(nao); dd.B.col = two(nao, 1, g_s); dd.B.bat.tab0 = tGm;
+      dd.C.ptr = X1; dd.C.row = lin(nao); dd.C.col = two(nao, 1, pe);
+      dd.C.bat.s0 = blk;
       // (e) Y2[kk][t][s][(i,n)][Q'] = sum_Q Y1[kk][t][s][Q][(i,n)] W(t)[Q][Q']
       ZGemm e;
       e.M = (int64_t)kbk * nao2; e.N = NQ; e.K = NQ;
@@ -234,16 +237,17 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
       e.B = dense(P0, NQ); e.B.bat.s1 = (int64_t)NQ * NQ;
       e.C.ptr = X2; e.C.row = two(nao2, NQ, blk); e.C.col = lin(1);
       e.C.bat.s1 = (int64_t)ns * pe; e.C.bat.s2 = pe;
-      // (f) Sigma[t][s][k][i][j] -= sum_{(n,Q')} Y2[kk][t][s][i][(n,Q')] conj(V(k,k-q)[Q'][j][n])
+      // (f) Sigma[t][s][k][i][j] -= sum_{(n,Q')} Y2[kk][t][s][i][(n,Q')] conj(V(k,k-q)[Q'][j][n]);
+      //     the (t,s) pairs are folded into the rows: M = nts*ns*nao rows ((t,s),i), N = nao, K = nao*NQ
       ZGemm f;
-      f.M = nao; f.N = nao; f.K = nao * NQ;
-      f.nb0 = kbk; f.nb1 = nts; f.nb2 = ns;
-      f.A.ptr = X2; f.A.row = lin(nao * NQ); f.A.col = lin(1);
-      f.A.bat.s0 = blk; f.A.bat.s1 = (int64_t)ns * pe; f.A.bat.s2 = pe;
+      f.M = (int64_t)nts * ns * nao; f.N = nao; f.K = nao * NQ;
+      f.nb0 = kbk;
+      f.A.ptr = X2; f.A.row = two(nao, nao * NQ, pe); f.A.col = lin(1);
+      f.A.bat.s0 = blk;
       f.B.ptr = c.V.get(); f.B.row = two(NQ, nao2, 1); f.B.col = lin(nao); f.B.conj = true;
       f.B.bat.tab0 = tVm;
-      f.C.ptr = Sigma + (int64_t)k0 * ge; f.C.row = lin(nao); f.C.col = lin(1);
-      f.C.bat.s0 = ge; f.C.bat.s1 = g_t; f.C.bat.s2 = g_s;
+      f.C.ptr = Sigma + (int64_t)k0 * ge; f.C.row = two(nao, nao, g_s); f.C.col = lin(1);
+      f.C.bat.s0 = ge;
       f.alpha = cmk(-1.0, 0.0); f.beta = cmk(1.0, 0.0);
       contract(dd);
       contract(e);

@@ -159,6 +159,7 @@ struct OperandSlices {
 struct GemmParams {
   int S;
   int BN;
+  int stages;
   int nkb;
   int ntiles_n;
   int64_t M, N;
@@ -195,16 +196,19 @@ struct SliceJob {
   int dep[3];
   int embed;                   // 1: left operand (doubled rows), 0: right operand
   int S;
-  int64_t rows_pad, kpad, e_ld;
+  int64_t rows_pad;            // real rows per plane
+  int64_t rpad;                // complex rows covered (rows_pad / 2 for the left operand)
+  int64_t kpad, e_ld;
   int8_t* out;
   int32_t* expo;
   bool r_fast;                 // consecutive threads walk rows (else K) when reading
 };
 
-constexpr int SL_ROWS = 32, SL_K = 32, SL_NT = 256;
+constexpr int TR = 32, TK = 64, SL_NT = 256;
+constexpr int EXP_EMPTY = -(1 << 30);
 
 __device__ __forceinline__ void enumerate_batch(const SliceJob& j, int64_t rb, int64_t& b0, int64_t& b1, int64_t& b2) {
-  // inverse of reduced_batch with non-dependent components set to 0
+  // inverse of reduced_batch with the components the operand does not depend on set to 0
   b0 = b1 = b2 = 0;
   int64_t r = rb;
   if (j.dep[2]) { b2 = r % j.n2; r /= j.n2; }
@@ -212,105 +216,145 @@ __device__ __forceinline__ void enumerate_batch(const SliceJob& j, int64_t rb, i
   if (j.dep[0]) { b0 = r; }
 }
 
-// One block handles SL_ROWS complex rows of one reduced batch: pass 1 finds the
-// per-row exponent, pass 2 writes the slice planes.
-__global__ void __launch_bounds__(SL_NT) slice_kernel(SliceJob j) {
-  __shared__ cplx tile[SL_ROWS][SL_K + 1];
-  __shared__ double rmax[SL_ROWS];
-  __shared__ int rexp[SL_ROWS];
-  __shared__ int64_t roff[SL_ROWS];
-  const int64_t rb = blockIdx.y;
-  const int64_t r0 = (int64_t)blockIdx.x * SL_ROWS;
+// Stage a TR x TK tile of the operand in shared memory (zero outside [0,R) x [0,K)).
+__device__ __forceinline__ void load_slice_tile(const SliceJob& j, const cplx* base, const int64_t* roff, int64_t r0,
+                                                int64_t kc, cplx (*tile)[TK + 1]) {
+  for (int e = threadIdx.x; e < TR * TK; e += SL_NT) {
+    int rl, kl;
+    if (j.r_fast) { rl = e % TR; kl = e / TR; } else { kl = e % TK; rl = e / TK; }
+    const int64_t r = r0 + rl, k = kc + kl;
+    cplx v = cmk(0.0, 0.0);
+    if (r < j.R && k < j.K) {
+      v = base[roff[rl] + j.kmap(j.k0 + k)];
+      if (j.conj) v.y = -v.y;
+    }
+    tile[rl][kl] = v;
+  }
+}
+
+// Pass 1: per-row exponent e (max |Re|,|Im| < 2^e) by atomicMax over K tiles.
+__global__ void __launch_bounds__(SL_NT) slice_expo_kernel(SliceJob j) {
+  __shared__ cplx tile[TR][TK + 1];
+  __shared__ int64_t roff[TR];
+  const int64_t rb = blockIdx.z, r0 = (int64_t)blockIdx.x * TR, kc = (int64_t)blockIdx.y * TK;
+  if (r0 >= j.R || kc >= j.K) return;
   int64_t b0, b1, b2;
   enumerate_batch(j, rb, b0, b1, b2);
   const cplx* base = j.ptr + j.bat(b0, b1, b2);
-  const int tid = threadIdx.x;
-  if (tid < SL_ROWS) {
-    int64_t r = r0 + tid;
-    roff[tid] = r < j.R ? j.rmap(r) : 0;
-    rmax[tid] = 0.0;
-  }
+  if (threadIdx.x < TR) roff[threadIdx.x] = (r0 + threadIdx.x < j.R) ? j.rmap(r0 + threadIdx.x) : 0;
   __syncthreads();
-  auto load_tile = [&](int64_t kc) {
-    for (int e = tid; e < SL_ROWS * SL_K; e += SL_NT) {
-      int rl, kl;
-      if (j.r_fast) { rl = e % SL_ROWS; kl = e / SL_ROWS; } else { kl = e % SL_K; rl = e / SL_K; }
-      int64_t r = r0 + rl, k = kc + kl;
-      cplx v = cmk(0.0, 0.0);
-      if (r < j.R && k < j.K) {
-        v = base[roff[rl] + j.kmap(j.k0 + k)];
-        if (j.conj) v.y = -v.y;
-      }
-      tile[rl][kl] = v;
-    }
-  };
-  // pass 1: row maxima
-  for (int64_t kc = 0; kc < j.K; kc += SL_K) {
-    load_tile(kc);
-    __syncthreads();
-    for (int e = tid; e < SL_ROWS * SL_K; e += SL_NT) {
-      int rl = e / SL_K, kl = e % SL_K;
-      cplx v = tile[rl][kl];
-      double m = fmax(fabs(v.x), fabs(v.y));
-      // warp lanes of one row: SL_K == 32 consecutive e share rl
-      for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-      if ((tid & 31) == 0) rmax[rl] = fmax(rmax[rl], m);
-    }
-    __syncthreads();
-  }
-  if (tid < SL_ROWS) {
-    int e = 0;
-    if (rmax[tid] > 0.0) frexp(rmax[tid], &e);  // rmax < 2^e
-    rexp[tid] = e;
-    int64_t r = r0 + tid;
-    if (r < j.R) j.expo[rb * j.e_ld + r] = e;
-  }
+  load_slice_tile(j, base, roff, r0, kc, tile);
   __syncthreads();
-  // pass 2: slices
+  // 8 threads per row, 8 columns each
+  const int rl = threadIdx.x / 8, part = threadIdx.x % 8;
+  double m = 0.0;
+#pragma unroll
+  for (int i = 0; i < TK / 8; ++i) {
+    cplx v = tile[rl][part * (TK / 8) + i];
+    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  }
+  for (int o = 4; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (part == 0 && m > 0.0 && r0 + rl < j.R) {
+    int e;
+    frexp(m, &e);
+    atomicMax(&j.expo[rb * j.e_ld + r0 + rl], e);
+  }
+}
+
+__device__ __forceinline__ void slice8(double x, int S, int8_t* q) {
+  // x = a * 2^(7-e), |x| < 128: truncation slices, exact in FP64
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    if (s < S) {
+      double t = trunc(x);
+      q[s] = (int8_t)(int)t;
+      x = (x - t) * 128.0;
+    }
+  }
+}
+
+// Pass 2: slice planes, including the zero padding of rows and K.
+__global__ void __launch_bounds__(SL_NT) slice_write_kernel(SliceJob j) {
+  __shared__ cplx tile[TR][TK + 1];
+  __shared__ int64_t roff[TR];
+  const int64_t rb = blockIdx.z, r0 = (int64_t)blockIdx.x * TR, kc = (int64_t)blockIdx.y * TK;
+  int64_t b0, b1, b2;
+  enumerate_batch(j, rb, b0, b1, b2);
+  const cplx* base = j.ptr + j.bat(b0, b1, b2);
+  if (threadIdx.x < TR) roff[threadIdx.x] = (r0 + threadIdx.x < j.R) ? j.rmap(r0 + threadIdx.x) : 0;
+  __syncthreads();
+  load_slice_tile(j, base, roff, r0, kc, tile);
+  __syncthreads();
+  const int rl = threadIdx.x / 8, grp = threadIdx.x % 8;
+  const int64_t r = r0 + rl;
+  const int64_t k = kc + grp * 8;  // first of 8 complex K positions
+  if (r >= j.rpad || 2 * k >= j.kpad) return;
+  int e = 0;
+  if (r < j.R) {
+    e = j.expo[rb * j.e_ld + r];
+    if (e == EXP_EMPTY) e = 0;
+  }
+  const double sc = ldexp(1.0, 7 - e);
+  int8_t qr[8][8], qi[8][8];  // [k][s]
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    cplx v = tile[rl][grp * 8 + i];
+    slice8(v.x * sc, j.S, qr[i]);
+    slice8(v.y * sc, j.S, qi[i]);
+  }
   const int64_t plane = j.rows_pad * j.kpad;
   int8_t* outb = j.out + rb * (int64_t)j.S * plane;
-  for (int64_t kc = 0; kc < j.K; kc += SL_K) {
-    load_tile(kc);
-    __syncthreads();
-    for (int e = tid; e < SL_ROWS * SL_K; e += SL_NT) {
-      int rl = e / SL_K, kl = e % SL_K;
-      int64_t r = r0 + rl, k = kc + kl;
-      if (r >= j.R || k >= j.K) continue;
-      cplx v = tile[rl][kl];
-      const int ex = rexp[rl];
-      double xr = ldexp(v.x, 7 - ex), xi = ldexp(v.y, 7 - ex);
-      for (int s = 0; s < j.S; ++s) {
-        double qr = trunc(xr), qi = trunc(xi);
-        int8_t ar = (int8_t)(int)qr, ai = (int8_t)(int)qi;
-        xr = (xr - qr) * 128.0;
-        xi = (xi - qi) * 128.0;
-        int8_t* p = outb + (int64_t)s * plane;
-        if (j.embed) {
-          int64_t row0 = 2 * r;
-          char2 w0 = make_char2(ar, (int8_t)(-ai));
-          char2 w1 = make_char2(ai, ar);
-          *reinterpret_cast<char2*>(p + row0 * j.kpad + 2 * k) = w0;
-          *reinterpret_cast<char2*>(p + (row0 + 1) * j.kpad + 2 * k) = w1;
-        } else {
-          *reinterpret_cast<char2*>(p + r * j.kpad + 2 * k) = make_char2(ar, ai);
-        }
+  for (int s = 0; s < j.S; ++s) {
+    int8_t* p = outb + (int64_t)s * plane;
+    if (j.embed) {
+      alignas(16) int8_t w0[16], w1[16];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        w0[2 * i] = qr[i][s];
+        w0[2 * i + 1] = (int8_t)(-qi[i][s]);
+        w1[2 * i] = qi[i][s];
+        w1[2 * i + 1] = qr[i][s];
       }
+      *reinterpret_cast<int4*>(p + (2 * r) * j.kpad + 2 * k) = *reinterpret_cast<int4*>(w0);
+      *reinterpret_cast<int4*>(p + (2 * r + 1) * j.kpad + 2 * k) = *reinterpret_cast<int4*>(w1);
+    } else {
+      alignas(16) int8_t w[16];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        w[2 * i] = qr[i][s];
+        w[2 * i + 1] = qi[i][s];
+      }
+      *reinterpret_cast<int4*>(p + r * j.kpad + 2 * k) = *reinterpret_cast<int4*>(w);
     }
-    __syncthreads();
   }
+}
+
+// exponent of a row that was entirely zero -> 0 (its slices are zero)
+__global__ void fix_empty_expo_kernel(int32_t* e, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (e[i] == EXP_EMPTY) e[i] = 0;
 }
 
 // ----------------------------------------------------------------------------
 // recombination epilogue (shared by both cores)
 // ----------------------------------------------------------------------------
+// 2^e as an exact double (e within the normal range)
+__device__ __forceinline__ double pow2(int e) {
+  e = max(-1022, min(1023, e));
+  return __longlong_as_double((long long)(e + 1023) << 52);
+}
+
+__device__ __forceinline__ void store_at(const GemmParams& p, cplx* dst, double re, double im, int ea, int eb) {
+  const double sc = pow2(ea + eb);
+  cplx v = cmul(p.alpha, cmk(re * sc, im * sc));
+  if (p.beta.x != 0.0 || p.beta.y != 0.0) v = cadd(v, cmul(p.beta, *dst));
+  *dst = v;
+}
+
 __device__ __forceinline__ void store_result(const GemmParams& p, int64_t b0, int64_t b1, int64_t b2, int64_t m, int64_t n,
                                              double re, double im, int ea, int eb) {
   cplx* Cb = p.C.ptr + p.C.bat(b0, b1, b2);
-  cplx* dst = Cb + p.C.row(m) + p.C.col(n);
-  cplx v = cmk(ldexp(re, ea + eb), ldexp(im, ea + eb));
-  v = cmul(p.alpha, v);
-  if (p.beta.x != 0.0 || p.beta.y != 0.0) v = cadd(v, cmul(p.beta, *dst));
-  *dst = v;
+  store_at(p, Cb + p.C.row(m) + p.C.col(n), re, im, ea, eb);
 }
 
 // ----------------------------------------------------------------------------
@@ -320,14 +364,18 @@ struct SmemLayout {
   int stage_bytes, a_plane_bytes, b_plane_bytes, stages;
 };
 
-__host__ __device__ inline SmemLayout smem_layout(int S, int BN) {
+__host__ __device__ inline SmemLayout smem_layout(int S, int BN, int stages) {
   SmemLayout L;
   L.a_plane_bytes = TILE_M * KBLK;
   L.b_plane_bytes = BN * KBLK;
   L.stage_bytes = S * (L.a_plane_bytes + L.b_plane_bytes);
-  L.stages = (SMEM_BUDGET - 2048) / L.stage_bytes;
-  if (L.stages > 6) L.stages = 6;
+  L.stages = stages;
   return L;
+}
+
+// bytes after the tile ring: barriers, TMEM slot, abort flag, exponents, C offsets
+__host__ __device__ inline int misc_bytes(int stages, int BN) {
+  return (2 * stages + 1) * 8 + 8 + (TILE_M / 2 + BN) * 4 + (TILE_M / 2 + BN) * 8 + 64;
 }
 
 __global__ void __launch_bounds__(NWARPS * 32, 1)
@@ -335,7 +383,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   // 1024-byte aligned base for the swizzled tiles
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const SmemLayout L = smem_layout(p.S, p.BN);
+  const SmemLayout L = smem_layout(p.S, p.BN, p.stages);
   uint8_t* tiles = smem;
   uint64_t* full_bar = reinterpret_cast<uint64_t*>(tiles + (size_t)L.stages * L.stage_bytes);
   uint64_t* empty_bar = full_bar + L.stages;
@@ -345,6 +393,8 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(misc + 4);
   int32_t* sh_eA = reinterpret_cast<int32_t*>(misc + 8);
   int32_t* sh_eB = sh_eA + TILE_M / 2;
+  int64_t* sh_rowC = reinterpret_cast<int64_t*>(misc + 8 + ((TILE_M / 2 + p.BN) * 4 + 7) / 8 * 8);
+  int64_t* sh_colC = sh_rowC + TILE_M / 2;
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int64_t bz = blockIdx.z;
@@ -367,14 +417,16 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   if (warp == 1) tmem_alloc(tmem_base_slot, ncols_alloc);
-  // exponents of this tile
+  // exponents and result offsets of this tile
   for (int i = threadIdx.x; i < TILE_M / 2 + p.BN; i += blockDim.x) {
     if (i < TILE_M / 2) {
       int64_t m = mrow0 / 2 + i;
       sh_eA[i] = m < p.M ? p.eA[rbA * p.eA_ld + m] : 0;
+      sh_rowC[i] = m < p.M ? p.C.row(m) : 0;
     } else {
       int64_t n = ncol0 + (i - TILE_M / 2);
       sh_eB[i - TILE_M / 2] = n < p.N ? p.eB[rbB * p.eB_ld + n] : 0;
+      sh_colC[i - TILE_M / 2] = n < p.N ? p.C.col(n) : 0;
     }
   }
   tc_fence_before();
@@ -469,15 +521,16 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
           int32_t q[16];
           tmem_ld16(tmem_base + ((uint32_t)(sp * 32) << 16) + (uint32_t)(d * p.BN + c0), q);
           tmem_wait_ld();
-          const double w = ldexp(1.0, -7 * (d + 2));
+          const double w = pow2(-7 * (d + 2));
 #pragma unroll
           for (int j = 0; j < 16; ++j) v[j] = fma((double)q[j], w, v[j]);
         }
+        cplx* Crow = p.C.ptr + p.C.bat(b0, b1, b2) + sh_rowC[row / 2];
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           double other = __shfl_xor_sync(0xffffffffu, v[j], 1);
           const int64_t n = ncol0 + c0 + j;
-          if (r == 0 && m < p.M && n < p.N) store_result(p, b0, b1, b2, m, n, v[j], other, ea, sh_eB[c0 + j]);
+          if (r == 0 && m < p.M && n < p.N) store_at(p, Crow + sh_colC[c0 + j], v[j], other, ea, sh_eB[c0 + j]);
         }
       }
     }
@@ -525,7 +578,7 @@ __global__ void split_gemm_ref_kernel(const int8_t* Ap, const int8_t* Bp, int64_
         acci += (int32_t)a1[k] * (int32_t)bb[k];
       }
     }
-    const double w = ldexp(1.0, -7 * (d + 2));
+    const double w = pow2(-7 * (d + 2));
     re = fma((double)accr, w, re);
     im = fma((double)acci, w, im);
   }
@@ -605,15 +658,46 @@ void split_release(Context& c) {
   c.split = nullptr;
 }
 
+namespace {
+
+__global__ void fill_int_kernel(int32_t* e, int64_t n, int32_t v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) e[i] = v;
+}
+
+// widest column tile for S diagonals in 512 TMEM columns, N a multiple of 16
+int max_bn(int S) {
+  int bn = (512 / S) / 16 * 16;
+  return std::min(bn, 256);
+}
+
+unsigned blocks_for(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)); }
+
+// Slice one operand (rows x K) into planes + exponents.
+void run_slicer(SliceJob& j, int64_t nrb, cudaStream_t st) {
+  const int64_t ne = nrb * j.e_ld;
+  fill_int_kernel<<<blocks_for(ne), 256, 0, st>>>(j.expo, ne, EXP_EMPTY);
+  GB_CHECK_LAUNCH();
+  require(nrb < 65536, GB200_ERR_INVALID, "split: too many operand batches");
+  dim3 g1((unsigned)((j.R + TR - 1) / TR), (unsigned)((j.K + TK - 1) / TK), (unsigned)nrb);
+  require(g1.y < 65536, GB200_ERR_INVALID, "split: contraction too long for the slicer grid");
+  slice_expo_kernel<<<g1, SL_NT, 0, st>>>(j);
+  GB_CHECK_LAUNCH();
+  dim3 g2((unsigned)((j.rpad + TR - 1) / TR), (unsigned)((j.kpad / 2 + TK - 1) / TK), (unsigned)nrb);
+  slice_write_kernel<<<g2, SL_NT, 0, st>>>(j);
+  GB_CHECK_LAUNCH();
+  fix_empty_expo_kernel<<<blocks_for(ne), 256, 0, st>>>(j.expo, ne);
+  GB_CHECK_LAUNCH();
+}
+
+}  // namespace
+
 void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st) {
   if (g0.M <= 0 || g0.N <= 0) return;
   validate(g0);
   const int S = c.slices;
   require(S >= 2 && S <= 8, GB200_ERR_INVALID, "split: slices out of range");
   require(g0.K > 0, GB200_ERR_INVALID, "split: empty contraction");
-  const int BN = (S <= 4) ? 128 : 64;
-  const SmemLayout L = smem_layout(S, BN);
-  require(L.stages >= 2, GB200_ERR_INVALID, "split: shared memory too small");
+  const int BN = std::min<int>(max_bn(S), (int)rup(g0.N, 16));
   // largest K chunk for which no INT32 diagonal can overflow: S * 2K * 127^2 < 2^31
   int64_t kmax = (int64_t)(2147483647.0 / (2.0 * 127.0 * 127.0 * S));
   kmax = kmax / 32 * 32;
@@ -634,35 +718,26 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st) {
     se.planesB.alloc((size_t)(nrbB * S * rowsB_pad * kpad));
     se.expA.alloc((size_t)(nrbA * rowsA_pad / 2));
     se.expB.alloc((size_t)(nrbB * rowsB_pad));
-    // padding rows and K tails must read as zero
-    GB_CUDA(cudaMemsetAsync(se.planesA.p, 0, (size_t)(nrbA * S * rowsA_pad * kpad), st));
-    GB_CUDA(cudaMemsetAsync(se.planesB.p, 0, (size_t)(nrbB * S * rowsB_pad * kpad), st));
     {
       SliceJob j{};
       j.ptr = g0.A.ptr; j.rmap = g0.A.row; j.kmap = g0.A.col; j.bat = g0.A.bat; j.conj = g0.A.conj;
       j.R = g0.M; j.K = Kc; j.k0 = k0; j.n0 = g0.nb0; j.n1 = g0.nb1; j.n2 = g0.nb2;
       std::copy(depA, depA + 3, j.dep);
-      j.embed = 1; j.S = S; j.rows_pad = rowsA_pad; j.kpad = kpad; j.e_ld = rowsA_pad / 2;
+      j.embed = 1; j.S = S; j.rows_pad = rowsA_pad; j.rpad = rowsA_pad / 2; j.kpad = kpad; j.e_ld = rowsA_pad / 2;
       j.out = se.planesA.p; j.expo = se.expA.p;
       j.r_fast = std::abs(g0.A.row.s_in) < std::abs(g0.A.col.s_in);
-      dim3 grid((unsigned)((g0.M + SL_ROWS - 1) / SL_ROWS), (unsigned)nrbA);
-      require(nrbA < 65536, GB200_ERR_INVALID, "split: too many batches");
-      slice_kernel<<<grid, SL_NT, 0, st>>>(j);
-      GB_CHECK_LAUNCH();
+      run_slicer(j, nrbA, st);
     }
     {
       SliceJob j{};
-      // right operand sliced per column: rows of the job are the N columns, K runs along B's rows
+      // right operand sliced per column: the job's rows are the N columns, K runs along B's rows
       j.ptr = g0.B.ptr; j.rmap = g0.B.col; j.kmap = g0.B.row; j.bat = g0.B.bat; j.conj = g0.B.conj;
       j.R = g0.N; j.K = Kc; j.k0 = k0; j.n0 = g0.nb0; j.n1 = g0.nb1; j.n2 = g0.nb2;
       std::copy(depB, depB + 3, j.dep);
-      j.embed = 0; j.S = S; j.rows_pad = rowsB_pad; j.kpad = kpad; j.e_ld = rowsB_pad;
+      j.embed = 0; j.S = S; j.rows_pad = rowsB_pad; j.rpad = rowsB_pad; j.kpad = kpad; j.e_ld = rowsB_pad;
       j.out = se.planesB.p; j.expo = se.expB.p;
       j.r_fast = std::abs(g0.B.col.s_in) < std::abs(g0.B.row.s_in);
-      dim3 grid((unsigned)((g0.N + SL_ROWS - 1) / SL_ROWS), (unsigned)nrbB);
-      require(nrbB < 65536, GB200_ERR_INVALID, "split: too many batches");
-      slice_kernel<<<grid, SL_NT, 0, st>>>(j);
-      GB_CHECK_LAUNCH();
+      run_slicer(j, nrbB, st);
     }
     GemmParams p{};
     p.S = S; p.BN = BN; p.nkb = (int)(kpad / KBLK);
@@ -685,11 +760,18 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st) {
       require(rowsA_total < (1LL << 31) && rowsB_total < (1LL << 31), GB200_ERR_INVALID, "split: operand too large for TMA");
       CUtensorMap mA = make_map(se.planesA.p, kpad, rowsA_total, TILE_M);
       CUtensorMap mB = make_map(se.planesB.p, kpad, rowsB_total, BN);
-      const size_t smem = (size_t)L.stages * L.stage_bytes + 1024 /*align*/ + 1024 /*barriers, exponents*/;
+      // pipeline depth: as many stages as the contraction has K blocks, within the shared-memory budget
+      const SmemLayout L1 = smem_layout(S, BN, 1);
+      int stages = (SMEM_BUDGET - 2048) / L1.stage_bytes;
+      stages = std::max(1, std::min({stages, 6, p.nkb}));
+      p.stages = stages;
+      const size_t smem = (size_t)stages * L1.stage_bytes + 1024 /*alignment*/ + misc_bytes(stages, BN);
       if (!se.attr_set) {
         GB_CUDA(cudaFuncSetAttribute(split_gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
         se.attr_set = true;
       }
+      require(smem <= 227 * 1024, GB200_ERR_INVALID, "split: shared memory budget exceeded");
+      require(rowsB_pad / BN < 65536 && rowsA_pad / TILE_M < 65536, GB200_ERR_INVALID, "split: grid too large");
       dim3 grid((unsigned)(rowsB_pad / BN), (unsigned)(rowsA_pad / TILE_M), (unsigned)nbatch);
       split_gemm_tc_kernel<<<grid, NWARPS * 32, smem, st>>>(mA, mB, p);
       GB_CHECK_LAUNCH();

@@ -148,15 +148,15 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
       const int64_t* tVp = c.tab_pair_plus.get() + (int64_t)q * nk + k0;
       const int64_t* tGp = c.tab_g_plus.get() + (int64_t)q * nk + k0;
       const int64_t blkT1 = (int64_t)nth * ns * pe;  // per kk in T1
-      // (a) T1[kk][t][s][(Q,p)][n] = sum_m V(k,k+q)[(Q,p)][m] G(t,s,k+q)[m][n]; the (t,s) pairs of
-      //     the first half of the grid are folded into the columns: one GEMM per k,
-      //     M = NQ*nao rows (Q,p), N = nth*ns*nao columns ((t,s),n), K = nao
+      // (a) T1[kk][t][s][(Q,p)][n] = sum_m V(k,k+q)[(Q,p)][m] G(t,s,k+q)[m][n], computed as its
+      //     transpose T1^T = G^T V^T so that the large operand V is the right (column) operand:
+      //     rows ((t,s),n) (M = nth*ns*nao), columns (Q,p) (N = NQ*nao), K = m
       ZGemm a;
-      a.M = (int64_t)NQ * nao; a.N = (int64_t)nth * ns * nao; a.K = nao;
+      a.M = (int64_t)nth * ns * nao; a.N = (int64_t)NQ * nao; a.K = nao;
       a.nb0 = kbk;
-      a.A = dense(c.V.get(), nao); a.A.bat.tab0 = tVp;
-      a.B.ptr = G; a.B.row = lin(nao); a.B.col = two(nao, 1, g_s); a.B.bat.tab0 = tGp;
-      a.C.ptr = X1; a.C.row = lin(nao); a.C.col = two(nao, 1, pe);
+      a.A.ptr = G; a.A.row = two(nao, 1, g_s); a.A.col = lin(nao); a.A.bat.tab0 = tGp;
+      a.B.ptr = c.V.get(); a.B.row = lin(1); a.B.col = lin(nao); a.B.bat.tab0 = tVp;
+      a.C.ptr = X1; a.C.row = two(nao, 1, pe); a.C.col = lin(nao);
       a.C.bat.s0 = blkT1;
       // (b) Bt[t][kk][s][Q][r][n] = sum_p Gbar(nts-1-t, s, k)[r][p] T1[kk][t][s][Q][p][n]
       ZGemm b;
@@ -168,15 +168,17 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
       b.B.bat.s0 = blkT1; b.B.bat.s1 = (int64_t)ns * pe; b.B.bat.s2 = pe;
       b.C.ptr = X2; b.C.row = lin(nao); b.C.col = two(nao, 1, nao2);
       b.C.bat.s0 = (int64_t)ns * pe; b.C.bat.s1 = (int64_t)kbk * ns * pe; b.C.bat.s2 = pe;
-      // (c) P0[t][Q][Q'] -= pref sum_{(kk,s),(r,n)} Bt[t][(kk,s)][Q][(r,n)] conj(V(k,k+q)[Q'][(r,n)])
+      // (c) P0[t][Q][Q'] -= pref sum_{(kk,s),(r,n)} Bt[t][(kk,s)][Q][(r,n)] conj(V(k,k+q)[Q'][(r,n)]),
+      //     computed as P0^T = conj(V) Bt^T: the tau-independent V is the left operand (sliced
+      //     once per call), Bt the right one; rows Q', columns Q, K = ((kk,s),(r,n))
       ZGemm cc;
       cc.M = NQ; cc.N = NQ; cc.K = (int64_t)kbk * ns * nao2;
       cc.nb0 = 1; cc.nb1 = 1; cc.nb2 = nth;
-      cc.A.ptr = X2; cc.A.row = lin(nao2); cc.A.col = two(nao2, 1, (int64_t)NQ * nao2);
-      cc.A.bat.s2 = (int64_t)kbk * ns * pe;
-      cc.B.ptr = c.V.get(); cc.B.row = twotab(nao2, 1, c.tab_pair_plus_ns.get() + ((int64_t)q * nk + k0) * ns);
-      cc.B.col = lin(nao2); cc.B.conj = true;
-      cc.C.ptr = P0; cc.C.row = lin(NQ); cc.C.col = lin(1); cc.C.bat.s2 = (int64_t)NQ * NQ;
+      cc.A.ptr = c.V.get(); cc.A.row = lin(nao2); cc.A.conj = true;
+      cc.A.col = twotab(nao2, 1, c.tab_pair_plus_ns.get() + ((int64_t)q * nk + k0) * ns);
+      cc.B.ptr = X2; cc.B.col = lin(nao2); cc.B.row = two(nao2, 1, (int64_t)NQ * nao2);
+      cc.B.bat.s2 = (int64_t)kbk * ns * pe;
+      cc.C.ptr = P0; cc.C.row = lin(1); cc.C.col = lin(NQ); cc.C.bat.s2 = (int64_t)NQ * NQ;
       cc.alpha = cmk(-pref, 0.0); cc.beta = cmk(1.0, 0.0);
       contract(a);
       contract(b);
@@ -219,34 +221,36 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
       const int64_t* tVm = c.tab_pair_minus.get() + (int64_t)q * nk + k0;
       const int64_t* tGm = c.tab_g_minus.get() + (int64_t)q * nk + k0;
       const int64_t blk = (int64_t)nts * ns * pe;  // per kk in Y1 / Y2
-      // (d) Y1[kk][t][s][(Q,i)][n] = sum_m V(k,k-q)[(Q,i)][m] G(t,s,k-q)[m][n]; (t,s) folded into
-      //     the columns as in (a)
+      // (d) Y1[kk][t][s][(Q,i)][n] = sum_m V(k,k-q)[(Q,i)][m] G(t,s,k-q)[m][n], as its transpose
+      //     (V the right operand): rows ((t,s),n), columns (Q,i), K = m
       ZGemm dd;
-      dd.M = (int64_t)NQ * nao; dd.N = (int64_t)nts * ns * nao; dd.K = nao;
+      dd.M = (int64_t)nts * ns * nao; dd.N = (int64_t)NQ * nao; dd.K = nao;
       dd.nb0 = kbk;
-      dd.A = dense(c.V.get(), nao); dd.A.bat.tab0 = tVm;
-      dd.B.ptr = G; dd.B.row = lin(nao); dd.B.col = two(nao, 1, g_s); dd.B.bat.tab0 = tGm;
-      dd.C.ptr = X1; dd.C.row = lin(nao); dd.C.col = two(nao, 1, pe);
+      dd.A.ptr = G; dd.A.row = two(nao, 1, g_s); dd.A.col = lin(nao); dd.A.bat.tab0 = tGm;
+      dd.B.ptr = c.V.get(); dd.B.row = lin(1); dd.B.col = lin(nao); dd.B.bat.tab0 = tVm;
+      dd.C.ptr = X1; dd.C.row = two(nao, 1, pe); dd.C.col = lin(nao);
       dd.C.bat.s0 = blk;
-      // (e) Y2[kk][t][s][(i,n)][Q'] = sum_Q Y1[kk][t][s][Q][(i,n)] W(t)[Q][Q']
+      // (e) Y2[kk][t][s][(i,n)][Q'] = sum_Q Y1[kk][t][s][Q][(i,n)] W(t)[Q][Q'], as Y2^T = W^T Y1:
+      //     the small W(t) is the left operand, Y1 the right one; rows Q', columns (kk,(i,n)), K = Q
       ZGemm e;
-      e.M = (int64_t)kbk * nao2; e.N = NQ; e.K = NQ;
+      e.M = NQ; e.N = (int64_t)kbk * nao2; e.K = NQ;
       e.nb0 = 1; e.nb1 = nts; e.nb2 = ns;
-      e.A.ptr = X1; e.A.row = two(nao2, 1, blk); e.A.col = lin(nao2);
-      e.A.bat.s1 = (int64_t)ns * pe; e.A.bat.s2 = pe;
-      e.B = dense(P0, NQ); e.B.bat.s1 = (int64_t)NQ * NQ;
-      e.C.ptr = X2; e.C.row = two(nao2, NQ, blk); e.C.col = lin(1);
+      e.A.ptr = P0; e.A.row = lin(1); e.A.col = lin(NQ); e.A.bat.s1 = (int64_t)NQ * NQ;
+      e.B.ptr = X1; e.B.row = lin(nao2); e.B.col = two(nao2, 1, blk);
+      e.B.bat.s1 = (int64_t)ns * pe; e.B.bat.s2 = pe;
+      e.C.ptr = X2; e.C.row = lin(1); e.C.col = two(nao2, NQ, blk);
       e.C.bat.s1 = (int64_t)ns * pe; e.C.bat.s2 = pe;
-      // (f) Sigma[t][s][k][i][j] -= sum_{(n,Q')} Y2[kk][t][s][i][(n,Q')] conj(V(k,k-q)[Q'][j][n]);
-      //     the (t,s) pairs are folded into the rows: M = nts*ns*nao rows ((t,s),i), N = nao, K = nao*NQ
+      // (f) Sigma[t][s][k][i][j] -= sum_{(n,Q')} Y2[kk][t][s][i][(n,Q')] conj(V(k,k-q)[Q'][j][n]), as
+      //     Sigma^T = conj(V) Y2^T: rows j (M = nao), columns ((t,s),i) (N = nts*ns*nao),
+      //     K = (n,Q'); the large Y2 is the right operand
       ZGemm f;
-      f.M = (int64_t)nts * ns * nao; f.N = nao; f.K = nao * NQ;
+      f.M = nao; f.N = (int64_t)nts * ns * nao; f.K = nao * NQ;
       f.nb0 = kbk;
-      f.A.ptr = X2; f.A.row = two(nao, nao * NQ, pe); f.A.col = lin(1);
-      f.A.bat.s0 = blk;
-      f.B.ptr = c.V.get(); f.B.row = two(NQ, nao2, 1); f.B.col = lin(nao); f.B.conj = true;
-      f.B.bat.tab0 = tVm;
-      f.C.ptr = Sigma + (int64_t)k0 * ge; f.C.row = two(nao, nao, g_s); f.C.col = lin(1);
+      f.A.ptr = c.V.get(); f.A.row = lin(nao); f.A.col = two(NQ, nao2, 1); f.A.conj = true;
+      f.A.bat.tab0 = tVm;
+      f.B.ptr = X2; f.B.row = lin(1); f.B.col = two(nao, nao * NQ, pe);
+      f.B.bat.s0 = blk;
+      f.C.ptr = Sigma + (int64_t)k0 * ge; f.C.row = lin(1); f.C.col = two(nao, nao, g_s);
       f.C.bat.s0 = ge;
       f.alpha = cmk(-1.0, 0.0); f.beta = cmk(1.0, 0.0);
       contract(dd);

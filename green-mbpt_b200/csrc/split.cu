@@ -39,8 +39,10 @@ namespace {
 
 constexpr int KBLK = 64;          // bytes of K per pipeline stage (one 64B swizzle atom)
 constexpr int TILE_M = 128;       // real rows per CTA (64 complex rows)
+constexpr int EPI_CH = 32;        // result columns staged per epilogue step
 constexpr int SMEM_BUDGET = 200 * 1024;
-constexpr int NWARPS = 6;
+constexpr int NWARPS = 10;        // producer, MMA, 8 epilogue warps
+constexpr int EPI_THREADS = 256;
 constexpr long long WAIT_LIMIT = 4000000000LL;  // clock64 cycles (~2 s)
 
 enum SplitErr { SERR_NONE = 0, SERR_TIMEOUT_PRODUCER = 1, SERR_TIMEOUT_MMA = 2, SERR_TIMEOUT_EPILOGUE = 3 };
@@ -58,6 +60,10 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_local(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
@@ -160,6 +166,9 @@ struct GemmParams {
   int S;
   int BN;
   int stages;
+  int rows_fast;  // result rows are the unit-stride index (write-out walks rows first)
+  int nbuf;       // TMEM accumulator sets (2: epilogue overlaps the next tile's MMAs)
+  int tiles_m, tiles_n;
   int nkb;
   int ntiles_n;
   int64_t M, N;
@@ -261,16 +270,27 @@ __global__ void __launch_bounds__(SL_NT) slice_expo_kernel(SliceJob j) {
   }
 }
 
-__device__ __forceinline__ void slice8(double x, int S, int8_t* q) {
-  // x = a * 2^(7-e), |x| < 128: truncation slices, exact in FP64
-#pragma unroll
-  for (int s = 0; s < 8; ++s) {
-    if (s < S) {
-      double t = trunc(x);
-      q[s] = (int8_t)(int)t;
-      x = (x - t) * 128.0;
-    }
-  }
+// Ozaki digits of one real number: with X = trunc(a * 2^(7S - e)) (exact conversion, |X| < 2^(7S)),
+// slice s is the s-th base-128 digit of |X| from the top, carrying the sign of a.  This equals
+// the truncation cascade q_s = trunc(x_s), x_{s+1} = 128 (x_s - q_s) with x_0 = a 2^(7-e).
+struct Digits {
+  uint64_t mag;
+  uint32_t neg;  // 0 or 0xFFFFFFFF
+};
+
+__device__ __forceinline__ Digits digits_of(double a, double scale) {
+  const long long X = __double2ll_rz(a * scale);
+  Digits d;
+  d.neg = X < 0 ? 0xFFFFFFFFu : 0u;
+  d.mag = (uint64_t)(X < 0 ? -X : X);
+  return d;
+}
+
+// signed digit s (top = 0) as a byte in the low 8 bits
+__device__ __forceinline__ uint32_t digit_byte(const Digits& d, int shift) {
+  uint32_t q = (uint32_t)(d.mag >> shift) & 127u;
+  q = (q ^ d.neg) - d.neg;  // conditional negate
+  return q & 0xFFu;
 }
 
 // Pass 2: slice planes, including the zero padding of rows and K.
@@ -294,37 +314,44 @@ __global__ void __launch_bounds__(SL_NT) slice_write_kernel(SliceJob j) {
     e = j.expo[rb * j.e_ld + r];
     if (e == EXP_EMPTY) e = 0;
   }
-  const double sc = ldexp(1.0, 7 - e);
-  int8_t qr[8][8], qi[8][8];  // [k][s]
+  const int S = j.S;
+  // 2^(7S - e) in two exact power-of-two factors (the exponent can exceed the double range
+  // for rows of tiny magnitude)
+  const int ex = 7 * S - e;
+  const int ex1 = max(-1000, min(1000, ex));
+  const double sc1 = __longlong_as_double((long long)(ex1 + 1023) << 52);
+  const double sc2 = __longlong_as_double((long long)(max(-1022, min(1023, ex - ex1)) + 1023) << 52);
+  Digits dr[8], di[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
-    cplx v = tile[rl][grp * 8 + i];
-    slice8(v.x * sc, j.S, qr[i]);
-    slice8(v.y * sc, j.S, qi[i]);
+    const cplx v = tile[rl][grp * 8 + i];
+    dr[i] = digits_of(v.x * sc1, sc2);
+    di[i] = digits_of(v.y * sc1, sc2);
   }
   const int64_t plane = j.rows_pad * j.kpad;
-  int8_t* outb = j.out + rb * (int64_t)j.S * plane;
-  for (int s = 0; s < j.S; ++s) {
+  int8_t* outb = j.out + rb * (int64_t)S * plane;
+  for (int s = 0; s < S; ++s) {
+    const int shift = 7 * (S - 1 - s);
+    uint32_t w0[4], w1[4];
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const uint32_t r0b = digit_byte(dr[2 * h], shift), i0b = digit_byte(di[2 * h], shift);
+      const uint32_t r1b = digit_byte(dr[2 * h + 1], shift), i1b = digit_byte(di[2 * h + 1], shift);
+      if (j.embed) {
+        // row 2r: (re, -im) pairs; row 2r+1: (im, re) pairs
+        const uint32_t ni0 = (0u - i0b) & 0xFFu, ni1 = (0u - i1b) & 0xFFu;
+        w0[h] = r0b | (ni0 << 8) | (r1b << 16) | (ni1 << 24);
+        w1[h] = i0b | (r0b << 8) | (i1b << 16) | (r1b << 24);
+      } else {
+        w0[h] = r0b | (i0b << 8) | (r1b << 16) | (i1b << 24);
+      }
+    }
     int8_t* p = outb + (int64_t)s * plane;
     if (j.embed) {
-      alignas(16) int8_t w0[16], w1[16];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        w0[2 * i] = qr[i][s];
-        w0[2 * i + 1] = (int8_t)(-qi[i][s]);
-        w1[2 * i] = qi[i][s];
-        w1[2 * i + 1] = qr[i][s];
-      }
-      *reinterpret_cast<int4*>(p + (2 * r) * j.kpad + 2 * k) = *reinterpret_cast<int4*>(w0);
-      *reinterpret_cast<int4*>(p + (2 * r + 1) * j.kpad + 2 * k) = *reinterpret_cast<int4*>(w1);
+      *reinterpret_cast<uint4*>(p + (2 * r) * j.kpad + 2 * k) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
+      *reinterpret_cast<uint4*>(p + (2 * r + 1) * j.kpad + 2 * k) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
     } else {
-      alignas(16) int8_t w[16];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        w[2 * i] = qr[i][s];
-        w[2 * i + 1] = qi[i][s];
-      }
-      *reinterpret_cast<int4*>(p + r * j.kpad + 2 * k) = *reinterpret_cast<int4*>(w);
+      *reinterpret_cast<uint4*>(p + r * j.kpad + 2 * k) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
     }
   }
 }
@@ -344,6 +371,20 @@ __device__ __forceinline__ double pow2(int e) {
   return __longlong_as_double((long long)(e + 1023) << 52);
 }
 
+// sum_d q_d 2^-7(d+2): exact in int64 while the digits cannot overflow it (S <= 5, |q_d| < 2^31),
+// then one rounding to double; FP64 accumulation in diagonal order beyond that.  Both engines
+// use this function, so they agree bit for bit.
+__device__ __forceinline__ double combine_diagonals(const int32_t* q, int S) {
+  if (S <= 5) {
+    long long acc = 0;
+    for (int d = 0; d < S; ++d) acc += (long long)q[d] << (7 * (S - 1 - d));
+    return (double)acc * pow2(-7 * (S + 1));
+  }
+  double v = 0.0;
+  for (int d = 0; d < S; ++d) v = fma((double)q[d], pow2(-7 * (d + 2)), v);
+  return v;
+}
+
 __device__ __forceinline__ void store_at(const GemmParams& p, cplx* dst, double re, double im, int ea, int eb) {
   const double sc = pow2(ea + eb);
   cplx v = cmul(p.alpha, cmk(re * sc, im * sc));
@@ -361,7 +402,7 @@ __device__ __forceinline__ void store_result(const GemmParams& p, int64_t b0, in
 // tcgen05 core
 // ----------------------------------------------------------------------------
 struct SmemLayout {
-  int stage_bytes, a_plane_bytes, b_plane_bytes, stages;
+  int stage_bytes, a_plane_bytes, b_plane_bytes, stages, ring_bytes, ctile_bytes;
 };
 
 __host__ __device__ inline SmemLayout smem_layout(int S, int BN, int stages) {
@@ -370,168 +411,257 @@ __host__ __device__ inline SmemLayout smem_layout(int S, int BN, int stages) {
   L.b_plane_bytes = BN * KBLK;
   L.stage_bytes = S * (L.a_plane_bytes + L.b_plane_bytes);
   L.stages = stages;
+  L.ring_bytes = stages * L.stage_bytes;
+  L.ctile_bytes = (TILE_M / 2) * EPI_CH * 16;
   return L;
 }
 
-// bytes after the tile ring: barriers, TMEM slot, abort flag, exponents, C offsets
+// bytes after the tile ring and the result tile: barriers, TMEM slot, flags, per-tile tables
 __host__ __device__ inline int misc_bytes(int stages, int BN) {
-  return (2 * stages + 1) * 8 + 8 + (TILE_M / 2 + BN) * 4 + (TILE_M / 2 + BN) * 8 + 64;
+  return (2 * stages + 4) * 8 + 16 + (TILE_M / 2 + BN) * 4 + (TILE_M / 2 + BN) * 8 + 64;
 }
 
+struct TileCoord {
+  int64_t b0, b1, b2, rbA, rbB, mrow0, ncol0;
+};
+
+__device__ __forceinline__ TileCoord tile_coord(const GemmParams& p, int64_t t) {
+  TileCoord c;
+  const int64_t per_batch = (int64_t)p.tiles_m * p.tiles_n;
+  const int64_t bz = t / per_batch;
+  const int64_t rem = t - bz * per_batch;
+  const int64_t by = rem / p.tiles_n, bx = rem - by * p.tiles_n;  // N fastest: neighbours share A
+  c.b2 = bz % p.nb2;
+  c.b1 = (bz / p.nb2) % p.nb1;
+  c.b0 = bz / (p.nb2 * p.nb1);
+  c.rbA = reduced_batch(p.depA, c.b0, c.b1, c.b2, p.nb1, p.nb2);
+  c.rbB = reduced_batch(p.depB, c.b0, c.b1, c.b2, p.nb1, p.nb2);
+  c.mrow0 = by * TILE_M;
+  c.ncol0 = bx * p.BN;
+  return c;
+}
+
+// Persistent tensor-core kernel: every CTA walks tiles blockIdx.x, +gridDim.x, ...
+//  warp 0       TMA producer (one thread), a ring of `stages` K blocks that runs across tiles
+//  warp 1       MMA issuer (one thread), `nbuf` TMEM accumulator sets of S * BN columns
+//  warps 2..5   epilogue: TMEM -> FP64 tile in shared memory -> coalesced global stores
+// With nbuf = 2 the epilogue of one tile overlaps the MMAs of the next.
+template <int SS>
 __global__ void __launch_bounds__(NWARPS * 32, 1)
     split_gemm_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, GemmParams p) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
-  // 1024-byte aligned base for the swizzled tiles
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const SmemLayout L = smem_layout(p.S, p.BN, p.stages);
   uint8_t* tiles = smem;
-  uint64_t* full_bar = reinterpret_cast<uint64_t*>(tiles + (size_t)L.stages * L.stage_bytes);
+  cplx* ctile = reinterpret_cast<cplx*>(smem + L.ring_bytes);
+  uint64_t* full_bar = reinterpret_cast<uint64_t*>(smem + L.ring_bytes + L.ctile_bytes);
   uint64_t* empty_bar = full_bar + L.stages;
-  uint64_t* accum_bar = empty_bar + L.stages;
-  uint8_t* misc = reinterpret_cast<uint8_t*>(accum_bar + 1);
+  uint64_t* accf_bar = empty_bar + L.stages;   // [2]
+  uint64_t* acce_bar = accf_bar + 2;           // [2]
+  uint8_t* misc = reinterpret_cast<uint8_t*>(acce_bar + 2);
   uint32_t* tmem_base_slot = reinterpret_cast<uint32_t*>(misc);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(misc + 4);
-  int32_t* sh_eA = reinterpret_cast<int32_t*>(misc + 8);
+  volatile int* epi_ok = reinterpret_cast<volatile int*>(misc + 8);
+  int32_t* sh_eA = reinterpret_cast<int32_t*>(misc + 16);
   int32_t* sh_eB = sh_eA + TILE_M / 2;
-  int64_t* sh_rowC = reinterpret_cast<int64_t*>(misc + 8 + ((TILE_M / 2 + p.BN) * 4 + 7) / 8 * 8);
+  int64_t* sh_rowC = reinterpret_cast<int64_t*>(misc + 16 + ((TILE_M / 2 + p.BN) * 4 + 7) / 8 * 8);
   int64_t* sh_colC = sh_rowC + TILE_M / 2;
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int64_t bz = blockIdx.z;
-  const int64_t b2 = bz % p.nb2, b1 = (bz / p.nb2) % p.nb1, b0 = bz / (p.nb2 * p.nb1);
-  const int64_t rbA = reduced_batch(p.depA, b0, b1, b2, p.nb1, p.nb2);
-  const int64_t rbB = reduced_batch(p.depB, b0, b1, b2, p.nb1, p.nb2);
-  const int64_t mrow0 = (int64_t)blockIdx.y * TILE_M;  // real rows
-  const int64_t ncol0 = (int64_t)blockIdx.x * p.BN;    // complex columns
-  const int S = p.S;
-  const uint32_t ncols_alloc = (S * p.BN <= 32) ? 32 : (S * p.BN <= 64) ? 64 : (S * p.BN <= 128) ? 128 : (S * p.BN <= 256) ? 256 : 512;
+  constexpr int S = SS;
+  const int nbuf = p.nbuf;
+  const uint32_t acc_cols = (uint32_t)(S * p.BN);
+  const uint32_t need = acc_cols * (uint32_t)nbuf;
+  const uint32_t ncols_alloc = need <= 32 ? 32 : need <= 64 ? 64 : need <= 128 ? 128 : need <= 256 ? 256 : 512;
+  const int64_t ntiles = (int64_t)p.tiles_m * p.tiles_n * p.nb0 * p.nb1 * p.nb2;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < L.stages; ++s) {
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
     }
-    mbar_init(accum_bar, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf_bar[b], 1);
+      mbar_init(&acce_bar[b], 1);
+    }
     *abort_flag = 0;
+    *epi_ok = 1;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   if (warp == 1) tmem_alloc(tmem_base_slot, ncols_alloc);
-  // exponents and result offsets of this tile
-  for (int i = threadIdx.x; i < TILE_M / 2 + p.BN; i += blockDim.x) {
-    if (i < TILE_M / 2) {
-      int64_t m = mrow0 / 2 + i;
-      sh_eA[i] = m < p.M ? p.eA[rbA * p.eA_ld + m] : 0;
-      sh_rowC[i] = m < p.M ? p.C.row(m) : 0;
-    } else {
-      int64_t n = ncol0 + (i - TILE_M / 2);
-      sh_eB[i - TILE_M / 2] = n < p.N ? p.eB[rbB * p.eB_ld + n] : 0;
-      sh_colC[i - TILE_M / 2] = n < p.N ? p.C.col(n) : 0;
-    }
-  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_base_slot;
 
-  int issued = 0;  // producer: number of stages issued
+  int64_t issued = 0;  // producer: K blocks issued in total
   if (warp == 0) {
     if (lane == 0) {
-      for (int kb = 0; kb < p.nkb; ++kb) {
-        const int st = kb % L.stages;
-        const uint32_t ph = (kb / L.stages) & 1;
-        if (kb >= L.stages) {
-          if (!mbar_wait(&empty_bar[st], ph ^ 1, abort_flag)) {
+      int64_t it = 0;
+      for (int64_t t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
+        const TileCoord tc = tile_coord(p, t);
+        for (int kb = 0; kb < p.nkb; ++kb, ++it) {
+          const int st = (int)(it % L.stages);
+          const uint32_t ph = (uint32_t)((it / L.stages) & 1);
+          if (it >= L.stages && !mbar_wait(&empty_bar[st], ph ^ 1, abort_flag)) {
             atomicExch(p.err, SERR_TIMEOUT_PRODUCER);
             *abort_flag = 1;
             break;
           }
+          uint8_t* sbase = tiles + (size_t)st * L.stage_bytes;
+          mbar_expect_tx(&full_bar[st], (uint32_t)L.stage_bytes);
+          for (int s = 0; s < S; ++s) {
+            const int ya = (int)((tc.rbA * S + s) * p.rowsA_pad + tc.mrow0);
+            tma_load_2d(sbase + s * L.a_plane_bytes, &mapA, kb * KBLK, ya, &full_bar[st]);
+          }
+          uint8_t* bbase = sbase + S * L.a_plane_bytes;
+          for (int u = 0; u < S; ++u) {
+            const int yb = (int)((tc.rbB * S + u) * p.rowsB_pad + tc.ncol0);
+            tma_load_2d(bbase + u * L.b_plane_bytes, &mapB, kb * KBLK, yb, &full_bar[st]);
+          }
+          issued = it + 1;
         }
-        uint8_t* sbase = tiles + (size_t)st * L.stage_bytes;
-        mbar_expect_tx(&full_bar[st], (uint32_t)L.stage_bytes);
-        for (int s = 0; s < S; ++s) {
-          const int ya = (int)((rbA * S + s) * p.rowsA_pad + mrow0);
-          tma_load_2d(sbase + s * L.a_plane_bytes, &mapA, kb * KBLK, ya, &full_bar[st]);
-        }
-        uint8_t* bbase = sbase + S * L.a_plane_bytes;
-        for (int t = 0; t < S; ++t) {
-          const int yb = (int)((rbB * S + t) * p.rowsB_pad + ncol0);
-          tma_load_2d(bbase + t * L.b_plane_bytes, &mapB, kb * KBLK, yb, &full_bar[st]);
-        }
-        issued = kb + 1;
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
       const uint32_t idesc = idesc_i8(p.BN);
-      bool ok = true;
-      for (int kb = 0; kb < p.nkb; ++kb) {
-        const int st = kb % L.stages;
-        const uint32_t ph = (kb / L.stages) & 1;
-        if (!mbar_wait(&full_bar[st], ph, abort_flag)) {
+      int64_t it = 0, tcount = 0;
+      for (int64_t t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x, ++tcount) {
+        const int buf = (int)(tcount % nbuf);
+        const int64_t use = tcount / nbuf;
+        if (use > 0 && !mbar_wait(&acce_bar[buf], (uint32_t)((use - 1) & 1), abort_flag)) {
           atomicExch(p.err, SERR_TIMEOUT_MMA);
           *abort_flag = 1;
-          ok = false;
           break;
         }
         tc_fence_after();
-        uint8_t* sbase = tiles + (size_t)st * L.stage_bytes;
-        uint8_t* bbase = sbase + S * L.a_plane_bytes;
-        for (int s = 0; s < S; ++s) {
-          const uint64_t ad = smem_desc_sw64(smem_u32(sbase + s * L.a_plane_bytes));
-          for (int t = 0; s + t < S; ++t) {
-            const uint64_t bd = smem_desc_sw64(smem_u32(bbase + t * L.b_plane_bytes));
-            const uint32_t dt = tmem_base + (uint32_t)((s + t) * p.BN);
+        const uint32_t acc = tmem_base + (uint32_t)buf * acc_cols;
+        bool ok = true;
+        for (int kb = 0; kb < p.nkb; ++kb, ++it) {
+          const int st = (int)(it % L.stages);
+          const uint32_t ph = (uint32_t)((it / L.stages) & 1);
+          if (!mbar_wait(&full_bar[st], ph, abort_flag)) {
+            atomicExch(p.err, SERR_TIMEOUT_MMA);
+            *abort_flag = 1;
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          uint8_t* sbase = tiles + (size_t)st * L.stage_bytes;
+          uint8_t* bbase = sbase + S * L.a_plane_bytes;
+          for (int s = 0; s < S; ++s) {
+            const uint64_t ad = smem_desc_sw64(smem_u32(sbase + s * L.a_plane_bytes));
+            for (int u = 0; s + u < S; ++u) {
+              const uint64_t bd = smem_desc_sw64(smem_u32(bbase + u * L.b_plane_bytes));
+              const uint32_t dt = acc + (uint32_t)((s + u) * p.BN);
 #pragma unroll
-            for (int kk = 0; kk < KBLK / 32; ++kk) {
-              // +32 bytes along K inside the swizzle atom = +2 in the encoded address
-              umma_i8(dt, ad + 2 * kk, bd + 2 * kk, idesc, (kb > 0 || kk > 0 || s > 0) ? 1u : 0u);
+              for (int kk = 0; kk < KBLK / 32; ++kk)
+                umma_i8(dt, ad + 2 * kk, bd + 2 * kk, idesc, (kb > 0 || kk > 0 || s > 0) ? 1u : 0u);
             }
           }
+          umma_commit(&empty_bar[st]);
         }
-        umma_commit(&empty_bar[st]);
+        if (!ok) break;
+        umma_commit(&accf_bar[buf]);
       }
-      if (ok) umma_commit(accum_bar);
     }
   } else {
-    // epilogue warps 2..5: TMEM sub-partition = warp % 4
+    // epilogue warps 2..9: TMEM sub-partition = warp % 4; the two warps of a sub-partition
+    // take alternate 16-column groups
     const int sp = warp % 4;
+    const int half = (warp - 2) / 4;
     const int row = sp * 32 + lane;  // real row inside the tile
-    bool ok = true;
-    if (lane == 0) {
-      ok = mbar_wait(accum_bar, 0, abort_flag);
-    }
-    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-    if (!ok) {
-      if (lane == 0) {
-        atomicExch(p.err, SERR_TIMEOUT_EPILOGUE);
-        *abort_flag = 1;
+    const int et = threadIdx.x - 64;  // 0..255
+    int64_t tcount = 0;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
+      const TileCoord tc = tile_coord(p, t);
+      const int buf = (int)(tcount % nbuf);
+      const int64_t use = tcount / nbuf;
+      // per-tile tables (the previous tile's write-out finished at the last barrier)
+      for (int i = et; i < TILE_M / 2 + p.BN; i += EPI_THREADS) {
+        if (i < TILE_M / 2) {
+          const int64_t m = tc.mrow0 / 2 + i;
+          sh_eA[i] = m < p.M ? p.eA[tc.rbA * p.eA_ld + m] : 0;
+          sh_rowC[i] = m < p.M ? p.C.row(m) : 0;
+        } else {
+          const int64_t n = tc.ncol0 + (i - TILE_M / 2);
+          sh_eB[i - TILE_M / 2] = n < p.N ? p.eB[tc.rbB * p.eB_ld + n] : 0;
+          sh_colC[i - TILE_M / 2] = n < p.N ? p.C.col(n) : 0;
+        }
       }
-    } else {
+      if (et == 0) {
+        const bool ok = mbar_wait(&accf_bar[buf], (uint32_t)(use & 1), abort_flag);
+        if (!ok) {
+          atomicExch(p.err, SERR_TIMEOUT_EPILOGUE);
+          *abort_flag = 1;
+        }
+        *epi_ok = ok ? 1 : 0;
+      }
+      // every epilogue thread reaches every named barrier, on the error path too
+      asm volatile("bar.sync 1, 256;" ::: "memory");
+      if (!*epi_ok) break;
       tc_fence_after();
-      const int64_t mreal = mrow0 + row;
-      const int64_t m = mreal / 2;
-      const int r = (int)(mreal & 1);
-      const int ea = sh_eA[row / 2];
-      for (int c0 = 0; c0 < p.BN; c0 += 16) {
-        double v[16];
+      const int mloc = row / 2;
+      const int r = row & 1;
+      const int ea = sh_eA[mloc];
+      // a warp whose 32 rows are all padding skips the accumulator reads
+      const bool live = tc.mrow0 + sp * 32 < 2 * p.M;
+      const uint32_t acc = tmem_base + (uint32_t)buf * acc_cols + ((uint32_t)(sp * 32) << 16);
+      const int64_t mlim = p.M - tc.mrow0 / 2, nlim = p.N - tc.ncol0;
+      cplx* Cb = p.C.ptr + p.C.bat(tc.b0, tc.b1, tc.b2);
+      const bool has_beta = p.beta.x != 0.0 || p.beta.y != 0.0;
+      for (int c0 = 0; c0 < p.BN; c0 += EPI_CH) {
+        const int cw = min(EPI_CH, p.BN - c0);
+        const int cc = half * 16;
+        if (live && cc < cw) {
+          // TMEM -> FP64 complex chunk: real rows write .x, imaginary rows .y.  The diagonals are
+          // combined exactly in int64 (S <= 5) or in FP64 in diagonal order, as combine_diagonals.
+          long long acc64[16];
+          double accd[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = 0.0;
-        for (int d = 0; d < S; ++d) {
-          int32_t q[16];
-          tmem_ld16(tmem_base + ((uint32_t)(sp * 32) << 16) + (uint32_t)(d * p.BN + c0), q);
-          tmem_wait_ld();
-          const double w = pow2(-7 * (d + 2));
+          for (int j = 0; j < 16; ++j) { acc64[j] = 0; accd[j] = 0.0; }
 #pragma unroll
-          for (int j = 0; j < 16; ++j) v[j] = fma((double)q[j], w, v[j]);
+          for (int d0 = 0; d0 < S; d0 += 4) {
+            int32_t q[4][16];
+#pragma unroll
+            for (int dd = 0; dd < 4; ++dd)
+              if (d0 + dd < S) tmem_ld16(acc + (uint32_t)((d0 + dd) * p.BN + c0 + cc), q[dd]);
+            tmem_wait_ld();
+#pragma unroll
+            for (int dd = 0; dd < 4; ++dd) {
+              if (d0 + dd < S) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                  if (S <= 5) acc64[j] += (long long)q[dd][j] << (7 * (S - 1 - (d0 + dd)));
+                  else accd[j] = fma((double)q[dd][j], pow2(-7 * (d0 + dd + 2)), accd[j]);
+                }
+              }
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const double v = (S <= 5 ? (double)acc64[j] * pow2(-7 * (S + 1)) : accd[j]) * pow2(ea + sh_eB[c0 + cc + j]);
+            reinterpret_cast<double*>(&ctile[mloc * EPI_CH + cc + j])[r] = v;
+          }
         }
-        cplx* Crow = p.C.ptr + p.C.bat(b0, b1, b2) + sh_rowC[row / 2];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          double other = __shfl_xor_sync(0xffffffffu, v[j], 1);
-          const int64_t n = ncol0 + c0 + j;
-          if (r == 0 && m < p.M && n < p.N) store_at(p, Crow + sh_colC[c0 + j], v[j], other, ea, sh_eB[c0 + j]);
+        const bool last = c0 + EPI_CH >= p.BN;
+        if (last) tc_fence_before();
+        asm volatile("bar.sync 1, 256;" ::: "memory");
+        if (last && et == 0) mbar_arrive_local(&acce_bar[buf]);  // this accumulator set may be reused
+        // coalesced write-out: consecutive threads walk the result index with unit stride
+        const int total = (TILE_M / 2) * cw;
+        for (int e = et; e < total; e += EPI_THREADS) {
+          int ml, nl;
+          if (p.rows_fast) { ml = e % (TILE_M / 2); nl = e / (TILE_M / 2); } else { nl = e % cw; ml = e / cw; }
+          if (ml >= mlim || c0 + nl >= nlim) continue;
+          cplx* dst = Cb + sh_rowC[ml] + sh_colC[c0 + nl];
+          cplx val = cmul(p.alpha, ctile[ml * EPI_CH + nl]);
+          if (has_beta) val = cadd(val, cmul(p.beta, *dst));
+          *dst = val;
         }
+        asm volatile("bar.sync 1, 256;" ::: "memory");
       }
     }
   }
@@ -539,9 +669,9 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
   __syncthreads();
   // after an abort, let in-flight TMA loads land before the shared memory is released
   if (warp == 0 && lane == 0 && *abort_flag) {
-    for (int kb = 0; kb < issued; ++kb) {
+    for (int64_t k = (issued > L.stages ? issued - L.stages : 0); k < issued; ++k) {
       long long t0 = clock64();
-      while (!mbar_try_wait(&full_bar[kb % L.stages], (kb / L.stages) & 1)) {
+      while (!mbar_try_wait(&full_bar[k % L.stages], (uint32_t)((k / L.stages) & 1))) {
         if (clock64() - t0 > WAIT_LIMIT) break;
       }
     }
@@ -565,7 +695,7 @@ __global__ void split_gemm_ref_kernel(const int8_t* Ap, const int8_t* Bp, int64_
   const int64_t n = (int64_t)blockIdx.x * 16 + threadIdx.x;
   if (m >= p.M || n >= p.N) return;
   const int S = p.S;
-  double re = 0.0, im = 0.0;
+  int32_t qr[8], qi[8];
   for (int d = 0; d < S; ++d) {
     int32_t accr = 0, acci = 0;
     for (int s = 0; s <= d; ++s) {
@@ -578,10 +708,10 @@ __global__ void split_gemm_ref_kernel(const int8_t* Ap, const int8_t* Bp, int64_
         acci += (int32_t)a1[k] * (int32_t)bb[k];
       }
     }
-    const double w = pow2(-7 * (d + 2));
-    re = fma((double)accr, w, re);
-    im = fma((double)acci, w, im);
+    qr[d] = accr;
+    qi[d] = acci;
   }
+  const double re = combine_diagonals(qr, S), im = combine_diagonals(qi, S);
   store_result(p, b0, b1, b2, m, n, re, im, p.eA[rbA * p.eA_ld + m], p.eB[rbB * p.eB_ld + n]);
 }
 
@@ -664,10 +794,10 @@ __global__ void fill_int_kernel(int32_t* e, int64_t n, int32_t v) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) e[i] = v;
 }
 
-// widest column tile for S diagonals in 512 TMEM columns, N a multiple of 16
-int max_bn(int S) {
-  int bn = (512 / S) / 16 * 16;
-  return std::min(bn, 256);
+// widest column tile for S diagonals in `cols` TMEM columns, a multiple of 16
+int max_bn(int S, int cols) {
+  int bn = (cols / S) / 16 * 16;
+  return std::max(16, std::min(bn, 256));
 }
 
 unsigned blocks_for(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)); }
@@ -697,7 +827,12 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st) {
   const int S = c.slices;
   require(S >= 2 && S <= 8, GB200_ERR_INVALID, "split: slices out of range");
   require(g0.K > 0, GB200_ERR_INVALID, "split: empty contraction");
-  const int BN = std::min<int>(max_bn(S), (int)rup(g0.N, 16));
+  // Short contractions (a few K blocks per tile) are epilogue-bound: two TMEM accumulator sets of
+  // S * BN <= 256 columns let the epilogue of one tile overlap the MMAs of the next.  Long
+  // contractions are MMA-bound: one set of up to 512 columns and wider tiles.
+  const bool short_k = rup(2 * std::min<int64_t>(g0.K, 1 << 20), KBLK) / KBLK <= 8;
+  const int nbuf = short_k ? 2 : 1;
+  const int BN = std::min<int>(max_bn(S, 512 / nbuf), (int)rup(g0.N, 16));
   // largest K chunk for which no INT32 diagonal can overflow: S * 2K * 127^2 < 2^31
   int64_t kmax = (int64_t)(2147483647.0 / (2.0 * 127.0 * 127.0 * S));
   kmax = kmax / 32 * 32;
@@ -748,6 +883,7 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st) {
     p.eA = se.expA.p; p.eB = se.expB.p; p.eA_ld = rowsA_pad / 2; p.eB_ld = rowsB_pad;
     p.C = g0.C; p.alpha = g0.alpha; p.beta = (k0 == 0) ? g0.beta : cmk(1.0, 0.0);
     p.err = se.err.p;
+    p.rows_fast = std::abs(g0.C.row.s_in) < std::abs(g0.C.col.s_in) ? 1 : 0;
     const int64_t nbatch = g0.nb0 * g0.nb1 * g0.nb2;
     require(nbatch < 65536, GB200_ERR_INVALID, "split: too many batches for one launch");
     if (se.core == 1) {
@@ -760,20 +896,40 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st) {
       require(rowsA_total < (1LL << 31) && rowsB_total < (1LL << 31), GB200_ERR_INVALID, "split: operand too large for TMA");
       CUtensorMap mA = make_map(se.planesA.p, kpad, rowsA_total, TILE_M);
       CUtensorMap mB = make_map(se.planesB.p, kpad, rowsB_total, BN);
-      // pipeline depth: as many stages as the contraction has K blocks, within the shared-memory budget
+      // TMA ring depth: what fits next to the result tile, at most 6 K blocks
       const SmemLayout L1 = smem_layout(S, BN, 1);
-      int stages = (SMEM_BUDGET - 2048) / L1.stage_bytes;
-      stages = std::max(1, std::min({stages, 6, p.nkb}));
+      int stages = (SMEM_BUDGET - L1.ctile_bytes - 4096) / L1.stage_bytes;
+      stages = std::max(1, std::min(stages, 6));
       p.stages = stages;
-      const size_t smem = (size_t)stages * L1.stage_bytes + 1024 /*alignment*/ + misc_bytes(stages, BN);
+      p.nbuf = nbuf;
+      p.tiles_m = (int)(rowsA_pad / TILE_M);
+      p.tiles_n = (int)(rowsB_pad / BN);
+      const SmemLayout Ls = smem_layout(S, BN, stages);
+      const size_t smem = (size_t)Ls.ring_bytes + Ls.ctile_bytes + 1024 /*alignment*/ + misc_bytes(stages, BN);
       if (!se.attr_set) {
-        GB_CUDA(cudaFuncSetAttribute(split_gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        const void* fns[] = {(const void*)split_gemm_tc_kernel<2>, (const void*)split_gemm_tc_kernel<3>,
+                             (const void*)split_gemm_tc_kernel<4>, (const void*)split_gemm_tc_kernel<5>,
+                             (const void*)split_gemm_tc_kernel<6>, (const void*)split_gemm_tc_kernel<7>,
+                             (const void*)split_gemm_tc_kernel<8>};
+        for (const void* f : fns)
+          GB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
         se.attr_set = true;
       }
       require(smem <= 227 * 1024, GB200_ERR_INVALID, "split: shared memory budget exceeded");
-      require(rowsB_pad / BN < 65536 && rowsA_pad / TILE_M < 65536, GB200_ERR_INVALID, "split: grid too large");
-      dim3 grid((unsigned)(rowsB_pad / BN), (unsigned)(rowsA_pad / TILE_M), (unsigned)nbatch);
-      split_gemm_tc_kernel<<<grid, NWARPS * 32, smem, st>>>(mA, mB, p);
+      // persistent launch: one CTA per SM walks the tiles
+      const int64_t ntiles = (int64_t)p.tiles_m * p.tiles_n * nbatch;
+      int nsm = 148;
+      GB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.device));
+      const unsigned grid = (unsigned)std::min<int64_t>(ntiles, nsm);
+      switch (S) {
+        case 2: split_gemm_tc_kernel<2><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+        case 3: split_gemm_tc_kernel<3><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+        case 4: split_gemm_tc_kernel<4><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+        case 5: split_gemm_tc_kernel<5><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+        case 6: split_gemm_tc_kernel<6><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+        case 7: split_gemm_tc_kernel<7><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+        default: split_gemm_tc_kernel<8><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+      }
       GB_CHECK_LAUNCH();
     }
   }

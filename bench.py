@@ -1,0 +1,414 @@
+"""Benchmark: GW self-consistency iterations per second on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config c2] [--slices 5]
+
+One step is one iteration of the self-consistency loop of mbpt.exe on the
+c2 workload (nk = 125 (5x5x5), nao = 40, naux = 250, ns = 1, ntau = 120,
+nw = 120, beta = 200, eps ~ U[-5,5] Ha): HF Fock build, GW self-energy
+(P0 -> W -> Sigma, split-precision contractions), chemical-potential search
+and Dyson step, energies.  Inputs are seeded synthetic data with the shapes and
+distributions of that configuration (no public dataset exists for it).
+
+Timing: W untimed warm-up steps, then K timed steps bracketed by a barrier and
+cudaDeviceSynchronize, CUDA events on the library's stream, max over ranks.
+`value` times the iteration with G already in HBM; `e2e` adds, every step, the
+copy of G from pinned host memory and the copy of the new G back.  G (384 MB)
+and V (100 GB) are larger than L2, so no flush is needed.
+
+With N > 1 (torchrun) the q loop is sharded across ranks and the partial
+self-energies are summed with an NCCL all-reduce before the Dyson step.
+
+--impl reference times the CPU oracle (numpy/BLAS restatement of the
+reference's gw_cpu_kernel, hf_cpu_kernels and dyson) on a bounded sample of the
+same workload on the host cores and extrapolates to one iteration.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "green-mbpt_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "GW iterations/s at nk=125,nao=40: split-prec vs FP64 on B200, max|ΔΣ|≤1e-8"
+UNIT = "iterations/s"
+WORKLOADS = {
+    "c2": "c2: nk=125 (5x5x5), nao=40, naux=250, ns=1, ntau=120, nw=120, beta=200, eps~U[-5,5]",
+    "c1": "c1: nk=64 (4x4x4), nao=26, naux=150, ns=2, ntau=100, beta=100, eps~U[-2,2]",
+    "c0": "c0: nk=8 (2x2x2), nao=10, naux=40, ns=1, ntau=60, beta=100, eps~U[-2,2]",
+}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return d.get("bf16_tflops_sustained", 1412.1), d.get("hbm_gbs", 6546.2), "measured"
+    return 1400.0, 6650.0, "fallback"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline(cfg: str, seed: int, nks: int = 3):
+    """Time the CPU oracle on a bounded sample and extrapolate to one iteration (seconds).
+
+    Sample: q = 0 with `nks` k-points for the polarization and the self-energy (work per
+    (q,k) is uniform, so the full cost is nk*nq/nks times it), the screened-interaction
+    solve of that q (times nq), the HF exchange row of one k (times nk*ns) and the Dyson
+    step and eigen-spectra of one k (times nk).
+    """
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import gw_oracle as O
+    from gb200 import synth
+
+    s = synth.make_config(cfg, seed=seed, with_integrals=False)
+    g = s.grid
+    rng = np.random.default_rng(seed + 1)
+    nk, ns, NQ, nts, nao = s.nk, s.ns, s.NQ, s.nts, s.nao
+    bz = O.NoSymBZ(s.mesh)
+    q = 0
+    ks = list(range(min(nks, nk)))
+    Vp = {k: synth.random_pair(rng, NQ, nao, hermitian=(bz.k1_from_k2q(k, q) == k)) for k in ks}
+    Vm = {k: synth.random_pair(rng, NQ, nao, hermitian=(bz.k2_from_k1q(k, q) == k)) for k in ks}
+    t0 = time.perf_counter()
+    P0 = np.zeros((nts, NQ, NQ), dtype=np.complex128)
+    for k in ks:
+        O.eval_P0_tilde(s.G, Vp[k], k, bz.k1_from_k2q(k, q), P0, ns)
+    t1 = time.perf_counter()
+    O.symmetrize_P0(P0, nk)
+    P = O.eval_P_tilde(P0, g.Tnt_b, g.Ttn_b)
+    t2 = time.perf_counter()
+    Sig = np.zeros_like(s.G)
+    for k in ks:
+        O.eval_selfenergy(s.G, Vm[k], k, bz.k2_from_k1q(k, q), P, Sig, ns)
+    t3 = time.perf_counter()
+    # HF exchange row of k = 0 over all k' (the dominant HF term)
+    dm = O.hf_density(s.G, ns)
+    th0 = time.perf_counter()
+    pref = 1.0 if ns == 2 else 0.5
+    Frow = np.zeros((nao, nao), dtype=np.complex128)
+    for kp in range(nk):
+        v = synth.random_pair(rng, NQ, nao)
+        vmm = v.reshape(NQ * nao, nao)
+        Y = (vmm @ dm[0, kp]).reshape(NQ, nao * nao)
+        Frow -= pref * (Y.T.copy().reshape(nao, nao * NQ) @ np.conj(vmm).T.copy().reshape(nao * NQ, nao)) / nk
+    th1 = time.perf_counter()
+    # Dyson step and eigen-spectra of one k
+    one = slice(0, 1)
+    F1 = np.zeros((ns, 1, nao, nao), dtype=np.complex128)
+    td0 = time.perf_counter()
+    O.selfenergy_eigenspectra(F1, Sig[:, :, one], s.F[:, one], s.S[:, one], g.Tnt_f)
+    O.compute_G(F1, Sig[:, :, one], s.F[:, one], s.S[:, one], 0.0, g.Tnt_f, g.Ttn_f, g.wsample_f)
+    td1 = time.perf_counter()
+    per_qk = ((t1 - t0) + (t3 - t2)) / len(ks)
+    est = per_qk * nk * nk + (t2 - t1) * nk + (th1 - th0) * nk * ns + (td1 - td0) * nk
+    sample_s = (t3 - t0) + (th1 - th0) + (td1 - td0)
+    desc = (f"q=0 with {len(ks)} of {nk} k for P0 and Sigma, W solve of that q, HF exchange row of one k, "
+            f"Dyson + eigen-spectra of one k; {sample_s:.1f} s measured, scaled by the uniform per-(q,k) work")
+    return est, desc, sample_s
+
+
+def blas_threads():
+    try:
+        from threadpoolctl import threadpool_info
+        n = [i.get("num_threads", 0) for i in threadpool_info() if i.get("user_api") == "blas"]
+        return max(n) if n else os.cpu_count()
+    except Exception:
+        return os.cpu_count()
+
+
+def setup_context(cfg, seed, slices, device, ws, rank):
+    from gb200 import lib, solvers, synth
+
+    s = synth.make_config(cfg, seed=seed, with_integrals=False)
+    g = s.grid
+    ctx = lib.Context(s.nk, s.nao, s.ns, s.NQ, g.nts, g.nw, g.nw_b, s.beta, device=device)
+    kp, km = solvers.kq_maps(s.mesh)
+    ctx.set_kq_maps(kp, km)
+    ctx.set_grid(g.Tnt_f, g.Ttn_f, g.Tnt_b, g.Ttn_b, g.wsample_f)
+    synth.upload_device_integrals(ctx, s.nk, s.NQ, s.nao, seed=seed, device=device)
+    ctx.set_hamiltonian(s.F, s.S)
+    ctx.set_precision(lib.PREC_SPLIT, slices)
+    if ws > 1:
+        per = (s.nk + ws - 1) // ws
+        ctx.set_q_range(min(s.nk, rank * per), min(s.nk, (rank + 1) * per))
+    return s, ctx
+
+
+def run_ours(args):
+    import torch
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(minutes=15))
+    from gb200 import lib
+
+    s, ctx = setup_context(args.config, args.seed, args.slices, local, ws, rank)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+    G0 = torch.from_numpy(s.G).pin_memory()
+    Gout = torch.empty_like(G0).pin_memory()
+    G = torch.empty(s.G.shape, dtype=torch.complex128, device=dev)
+    S1 = torch.zeros((s.ns, s.nk, s.nao, s.nao), dtype=torch.complex128, device=dev)
+    St = torch.zeros(s.G.shape, dtype=torch.complex128, device=dev)
+    Sdev = torch.from_numpy(s.S).to(dev)
+    dm = torch.empty_like(S1)
+    nel = s.nel_from_G0()
+    tol, mad = 1e-9, 0.0
+    state = {"mu": 0.0, "E": None}
+
+    def iteration():
+        if ws == 1:
+            state["mu"], state["E"] = ctx.iteration_device(G.data_ptr(), S1.data_ptr(), St.data_ptr(), mad, nel, tol,
+                                                           0.0, stream=sptr)
+            return
+        # q-sharded GW: partial self-energies are summed before the Dyson step
+        dm.copy_(G[-1] * (-1.0 if s.ns == 2 else -2.0))
+        ctx.hf_fock_device(dm.data_ptr(), Sdev.data_ptr(), mad, S1.data_ptr(), stream=sptr)
+        ctx.gw_sigma_device(G.data_ptr(), St.data_ptr(), stream=sptr)
+        dist.all_reduce(torch.view_as_real(St))
+        state["mu"] = ctx.dyson_solve_device(S1.data_ptr(), St.data_ptr(), nel, tol, 0.0, G.data_ptr(), stream=sptr)
+        state["E"] = ctx.energy_device(G.data_ptr(), S1.data_ptr(), St.data_ptr(), stream=sptr)
+
+    def step(ev=None):
+        if ev:
+            ev[0].record(stream)
+        G.copy_(G0, non_blocking=True)
+        if ev:
+            ev[1].record(stream)
+        iteration()
+        if ev:
+            ev[2].record(stream)
+        Gout.copy_(G, non_blocking=True)
+        if ev:
+            ev[3].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ctx.stats_enable(True)
+    launches0 = ctx.stats_read()[0]
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    for k in range(args.steps):
+        step(evs[k])
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches1, tc_n, tc_ms, tc_fl = ctx.stats_read()
+    ctx.stats_enable(False)
+    comp_ms = sum(e[1].elapsed_time(e[2]) for e in evs)
+    tot_ms = sum(e[0].elapsed_time(e[3]) for e in evs)
+    gw_ms = ctx.last_timings()["total"]
+    if dist:
+        t = torch.tensor([comp_ms, tot_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        comp_ms, tot_ms = float(t[0]), float(t[1])
+    return s, ctx, dict(comp_ms=comp_ms, tot_ms=tot_ms, gw_ms=gw_ms, clocks=clk, launches=launches1 - launches0,
+                        tc_n=tc_n, tc_ms=tc_ms, tc_fl=tc_fl, E=state["E"], mu=state["mu"],
+                        bytes_io=G0.numel() * 16, ws=ws, rank=rank, dist=dist, G0=G0, G=G, St=St, sptr=sptr)
+
+
+def fp64_sample(s, ctx, r, nq_sample):
+    """FP64 vs split GW on the q-points [0, nq_sample) from G0: time per q and max|dSigma|."""
+    import torch
+    from gb200 import lib
+
+    G = r["G"]
+    G.copy_(r["G0"])
+    torch.cuda.synchronize()
+    ctx.set_q_range(0, nq_sample)
+    out = {}
+    for name, mode in (("split", lib.PREC_SPLIT), ("fp64", lib.PREC_FP64)):
+        ctx.set_precision(mode, r["slices"])
+        Sig = torch.empty_like(r["St"])
+        ctx.gw_sigma_device(G.data_ptr(), Sig.data_ptr(), stream=r["sptr"])  # warm
+        torch.cuda.synchronize()
+        ctx.gw_sigma_device(G.data_ptr(), Sig.data_ptr(), stream=r["sptr"])
+        torch.cuda.synchronize()
+        out[name] = (Sig, ctx.last_timings()["total"])
+    ctx.set_precision(lib.PREC_SPLIT, r["slices"])
+    ctx.set_q_range(0, s.nk)
+    d = (out["split"][0] - out["fp64"][0]).abs().max().item()
+    return out["fp64"][1] / nq_sample, out["split"][1] / nq_sample, d, out["fp64"][0].abs().max().item()
+
+
+def main_ours(args):
+    s, ctx, r = run_ours(args)
+    r["slices"] = args.slices
+    ws, rank = r["ws"], r["rank"]
+    K = args.steps
+    comp_s = r["comp_ms"] / 1e3 / K
+    tot_s = r["tot_ms"] / 1e3 / K
+    line = None
+    if rank == 0:
+        bf16_peak, hbm_peak, peak_src = measured_peaks()
+        achieved = (r["tc_fl"] / (r["tc_ms"] / 1e3) / 1e12) if r["tc_ms"] > 0 else None
+        fp64_q, split_q, dsig, smax = (None, None, None, None)
+        if ws == 1 and not args.no_fp64_sample:
+            fp64_q, split_q, dsig, smax = fp64_sample(s, ctx, r, args.fp64_q)
+        fp64_iter = None
+        if fp64_q is not None:
+            # the FP64 path differs from the split one only inside the GW contractions
+            fp64_iter = comp_s - r["gw_ms"] / 1e3 + fp64_q / 1e3 * s.nk
+        cpu_est, cpu_desc, _ = cpu_baseline(args.config, args.seed)
+        line = {
+            "metric": METRIC, "value": 1.0 / comp_s, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": args.warmup,
+            "ms_per_step": comp_s * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded generator; V generated on the GPU)",
+            "config": {"workload": WORKLOADS[args.config], "precision": f"split, {args.slices} INT8 slices",
+                       "parallelism": f"q-sharded over {ws} GPU(s), NCCL all-reduce of Sigma" if ws > 1 else "1 GPU",
+                       "l2": "inputs larger than L2 (G 384 MB, V 100 GB): no flush"},
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": bf16_peak, "unit": "TFLOP/s",
+                         "frac": (achieved / bf16_peak) if achieved else None, "traffic": None,
+                         "kernel": "split_gemm_tc_kernel (tcgen05 kind::i8)", "launches": r["tc_n"],
+                         "peak_source": f"{peak_src} bf16 dense sustained; achieved counts FP64-equivalent complex flops"},
+            "cpu_baseline": {"value": 1.0 / cpu_est, "unit": UNIT, "cores": blas_threads(), "kind": "port",
+                             "sample": cpu_desc},
+            "e2e": {"value": 1.0 / tot_s, "unit": UNIT, "h2d_bytes_per_step": r["bytes_io"],
+                    "d2h_bytes_per_step": r["bytes_io"]},
+            "clocks": r["clocks"], "gpu_launches": r["launches"],
+            "energies": {"E_1b": r["E"][0], "E_HF": r["E"][1], "E_corr": r["E"][2], "mu": r["mu"]} if r["E"] else None,
+        }
+        if fp64_iter is not None:
+            line["fp64_gpu"] = {"value": 1.0 / fp64_iter, "unit": UNIT,
+                                "estimate": f"FP64 GW timed on q-points [0,{args.fp64_q}) x {s.nk}, rest of the iteration measured"}
+            line["split_vs_fp64"] = fp64_iter / comp_s
+            line["accuracy"] = {"max_abs_dSigma_sample": dsig, "max_abs_Sigma_sample": smax,
+                                "sample": f"partial Sigma of q-points [0,{args.fp64_q}), split vs FP64 GPU"}
+        print(json.dumps(line), flush=True)
+    if r["dist"]:
+        r["dist"].barrier()
+        r["dist"].destroy_process_group()
+    ctx.close()
+    return line
+
+
+def main_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return None  # the CPU reference runs on rank 0 only
+    for _ in range(args.warmup):
+        cpu_baseline(args.config, args.seed)
+    ests, desc = [], ""
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        est, desc, _ = cpu_baseline(args.config, args.seed)
+        ests.append(est)
+    wall = time.perf_counter() - t0
+    v = 1.0 / statistics.mean(ests)
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * statistics.mean(ests), "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)", "impl": "reference",
+        "config": {"workload": WORKLOADS[args.config], "precision": "FP64 (CPU oracle restating the reference kernels)"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": blas_threads(), "kind": "port", "sample": desc,
+                         "sample_wall_s": wall / max(1, args.steps)},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return line
+
+
+def parse(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(WORKLOADS), default="c2")
+    ap.add_argument("--slices", type=int, default=5)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--fp64-q", dest="fp64_q", type=int, default=1, help="q-points timed for the FP64 comparison")
+    ap.add_argument("--no-fp64-sample", action="store_true")
+    a = ap.parse_args(argv)
+    if a.warmup < 3:
+        ap.error("at least 3 warm-up steps")
+    return a
+
+
+if __name__ == "__main__":
+    args = parse()
+    if args.impl == "reference":
+        main_reference(args)
+    else:
+        main_ours(args)

@@ -11,6 +11,10 @@
 
 using namespace gb200;
 
+namespace gb200 {
+std::atomic<long long> g_launch_count{0};
+}
+
 namespace {
 
 thread_local std::string g_create_error;
@@ -61,22 +65,34 @@ __global__ void scatter_pairs_kernel(const cplx* half_chunk, int64_t p0, int64_t
   }
 }
 
-void upload_integrals(Context& c, DevArray<cplx>& dst, const double* V_half, int64_t npairs) {
+void upload_integrals(Context& c, DevArray<cplx>& dst, const double* V_half, int64_t npairs, bool on_device,
+                      cudaStream_t st) {
   const int nk = c.d.nk;
   const int64_t pe = c.pair_elems();
   require(npairs == (int64_t)nk * (nk + 1) / 2, GB200_ERR_INVALID, "set_integrals: npairs must be nk(nk+1)/2");
   dst.alloc((size_t)nk * nk * pe);
-  // stream the half storage through a bounded staging buffer
+  const cplx* src = reinterpret_cast<const cplx*>(V_half);
+  if (on_device) {
+    // the half storage is already on the GPU: scatter it in place, chunk by chunk
+    const int64_t chunk_pairs = std::max<int64_t>(1, std::min<int64_t>(npairs, (int64_t)(4e9 / (pe * sizeof(cplx)))));
+    for (int64_t p0 = 0; p0 < npairs; p0 += chunk_pairs) {
+      int64_t cnt = std::min(chunk_pairs, npairs - p0);
+      scatter_pairs_kernel<<<148 * 16, 256, 0, st>>>(src + p0 * pe, p0, cnt, dst.p, nk, c.d.NQ, c.d.nao);
+      GB_CHECK_LAUNCH();
+    }
+    GB_CUDA(cudaStreamSynchronize(st));
+    return;
+  }
+  // stream the host half storage through a bounded staging buffer
   const int64_t chunk_pairs = std::max<int64_t>(1, std::min<int64_t>(npairs, (int64_t)(1e9 / (pe * sizeof(cplx)))));
   DevArray<cplx> stage;
   stage.alloc((size_t)chunk_pairs * pe);
   for (int64_t p0 = 0; p0 < npairs; p0 += chunk_pairs) {
     int64_t cnt = std::min(chunk_pairs, npairs - p0);
-    GB_CUDA(cudaMemcpyAsync(stage.p, reinterpret_cast<const cplx*>(V_half) + p0 * pe,
-                            (size_t)cnt * pe * sizeof(cplx), cudaMemcpyHostToDevice, c.stream));
-    scatter_pairs_kernel<<<148 * 16, 256, 0, c.stream>>>(stage.p, p0, cnt, dst.p, nk, c.d.NQ, c.d.nao);
+    GB_CUDA(cudaMemcpyAsync(stage.p, src + p0 * pe, (size_t)cnt * pe * sizeof(cplx), cudaMemcpyHostToDevice, st));
+    scatter_pairs_kernel<<<148 * 16, 256, 0, st>>>(stage.p, p0, cnt, dst.p, nk, c.d.NQ, c.d.nao);
     GB_CHECK_LAUNCH();
-    GB_CUDA(cudaStreamSynchronize(c.stream));
+    GB_CUDA(cudaStreamSynchronize(st));
   }
 }
 
@@ -149,6 +165,10 @@ void gb200_destroy(gb200_context* ctx) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   split_release(*c);
+  for (auto& r : c->records) {
+    if (r.start) cudaEventDestroy(r.start);
+    if (r.stop) cudaEventDestroy(r.stop);
+  }
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -195,11 +215,11 @@ int gb200_set_integrals(gb200_context* ctx, int which, const double* V_half, int
   return guarded(ctx, [&](Context& c) {
     require(V_half != nullptr, GB200_ERR_INVALID, "set_integrals: null pointer");
     if (which == GB200_INTEGRALS_GW) {
-      upload_integrals(c, c.V, V_half, npairs);
+      upload_integrals(c, c.V, V_half, npairs, false, c.stream);
       c.have_V = true;
       split_invalidate(c);
     } else if (which == GB200_INTEGRALS_HF) {
-      upload_integrals(c, c.Vhf, V_half, npairs);
+      upload_integrals(c, c.Vhf, V_half, npairs, false, c.stream);
       c.have_Vhf = true;
     } else {
       throw Error(GB200_ERR_INVALID, "set_integrals: unknown integral set");
@@ -376,6 +396,97 @@ int gb200_last_timings(const gb200_context* ctx, float* out4) {
   if (!c || !out4) return GB200_ERR_INVALID;
   std::memcpy(out4, c->timings, sizeof(c->timings));
   return GB200_OK;
+}
+
+int gb200_set_integrals_device(gb200_context* ctx, int which, const double* V_dev, int64_t pair_begin,
+                               int64_t pair_count, void* stream) {
+  return guarded(ctx, [&](Context& c) {
+    require(V_dev != nullptr, GB200_ERR_INVALID, "set_integrals_device: null pointer");
+    require(which == GB200_INTEGRALS_GW || which == GB200_INTEGRALS_HF, GB200_ERR_INVALID,
+            "set_integrals_device: unknown integral set");
+    const int nk = c.d.nk;
+    const int64_t npairs = (int64_t)nk * (nk + 1) / 2;
+    require(pair_begin >= 0 && pair_count > 0 && pair_begin + pair_count <= npairs, GB200_ERR_INVALID,
+            "set_integrals_device: pair range outside [0, nk(nk+1)/2)");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+    DevArray<cplx>& dst = which == GB200_INTEGRALS_GW ? c.V : c.Vhf;
+    int64_t& done = which == GB200_INTEGRALS_GW ? c.pairs_set_gw : c.pairs_set_hf;
+    const int64_t pe = c.pair_elems();
+    if (pair_begin == 0) done = 0;
+    dst.alloc((size_t)nk * nk * pe);
+    scatter_pairs_kernel<<<148 * 16, 256, 0, st>>>(reinterpret_cast<const cplx*>(V_dev), pair_begin, pair_count, dst.p,
+                                                   nk, c.d.NQ, c.d.nao);
+    GB_CHECK_LAUNCH();
+    GB_CUDA(cudaStreamSynchronize(st));
+    done += pair_count;
+    if (which == GB200_INTEGRALS_GW) {
+      c.have_V = done >= npairs;
+      split_invalidate(c);
+    } else {
+      c.have_Vhf = done >= npairs;
+    }
+  });
+}
+
+int gb200_set_q_range(gb200_context* ctx, int q_begin, int q_end) {
+  return guarded(ctx, [&](Context& c) {
+    require(q_begin >= 0 && q_end <= c.d.nk && q_begin <= q_end, GB200_ERR_INVALID, "set_q_range: need 0 <= begin <= end <= nk");
+    c.q_begin = q_begin;
+    c.q_end = q_end;
+  });
+}
+
+int gb200_dyson_solve_device(gb200_context* ctx, double* Sigma1_dev, double* Sigma_dev, double nel_target, double tol,
+                             double* mu_inout, double* G_dev, void* stream) {
+  return guarded(ctx, [&](Context& c) {
+    require(Sigma1_dev && Sigma_dev && mu_inout && G_dev, GB200_ERR_INVALID, "dyson_solve_device: null pointer");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+    cplx* S1 = reinterpret_cast<cplx*>(Sigma1_dev);
+    cplx* St = reinterpret_cast<cplx*>(Sigma_dev);
+    double mu = *mu_inout;
+    if (nel_target > 0) {
+      dyson_prepare_X(c, S1, St, false, st);
+      mu = dyson_find_mu(c, mu, nel_target, tol, nullptr, st);
+    }
+    dyson_compute_G(c, S1, St, mu, reinterpret_cast<cplx*>(G_dev), st);
+    GB_CUDA(cudaStreamSynchronize(st));
+    *mu_inout = mu;
+  });
+}
+
+int gb200_energy_device(gb200_context* ctx, const double* G_dev, const double* Sigma1_dev, const double* Sigma_dev,
+                        double* e_out3, void* stream) {
+  return guarded(ctx, [&](Context& c) {
+    require(G_dev && Sigma1_dev && Sigma_dev && e_out3, GB200_ERR_INVALID, "energy_device: null pointer");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+    energy(c, reinterpret_cast<const cplx*>(G_dev), reinterpret_cast<const cplx*>(Sigma1_dev),
+           reinterpret_cast<const cplx*>(Sigma_dev), e_out3, st);
+  });
+}
+
+int gb200_stats_enable(gb200_context* ctx, int on) {
+  return guarded(ctx, [&](Context& c) {
+    c.stats_on = on != 0;
+    c.records_used = 0;
+  });
+}
+
+int gb200_stats_read(gb200_context* ctx, long long* launches_total, long long* tc_launches, double* tc_ms,
+                     double* tc_alg_flops) {
+  return guarded(ctx, [&](Context& c) {
+    double ms = 0.0, fl = 0.0;
+    for (size_t i = 0; i < c.records_used; ++i) {
+      GB_CUDA(cudaEventSynchronize(c.records[i].stop));
+      float t = 0.f;
+      GB_CUDA(cudaEventElapsedTime(&t, c.records[i].start, c.records[i].stop));
+      ms += t;
+      fl += c.records[i].alg_flops;
+    }
+    if (launches_total) *launches_total = g_launch_count.load();
+    if (tc_launches) *tc_launches = (long long)c.records_used;
+    if (tc_ms) *tc_ms = ms;
+    if (tc_alg_flops) *tc_alg_flops = fl;
+  });
 }
 
 }  // extern "C"

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cuComplex.h>
 
+#include <atomic>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -41,7 +42,14 @@ struct Error : std::runtime_error {
     }                                                                                                \
   } while (0)
 
-#define GB_CHECK_LAUNCH() GB_CUDA(cudaGetLastError())
+// Every kernel launch of the library goes through this check, which also counts it
+// (gb200_kernel_stats reports the count).
+extern std::atomic<long long> g_launch_count;
+#define GB_CHECK_LAUNCH()                                \
+  do {                                                   \
+    ::gb200::g_launch_count.fetch_add(1, std::memory_order_relaxed); \
+    GB_CUDA(cudaGetLastError());                         \
+  } while (0)
 
 inline void require(bool cond, int code, const std::string& msg) {
   if (!cond) throw Error(code, msg);

@@ -59,6 +59,13 @@ enum ScratchSlot {
 
 struct SplitEngine;
 
+// One timed launch of the tensor-core contraction kernel (CUDA events on its stream)
+// with the FP64-equivalent complex flops of the contraction it performed.
+struct KernelRecord {
+  cudaEvent_t start = nullptr, stop = nullptr;
+  double alg_flops = 0.0;
+};
+
 struct Context {
   gb200_dims d{};
   int device = 0;
@@ -88,6 +95,14 @@ struct Context {
 
   Scratch scratch;
   float timings[4] = {0, 0, 0, 0};
+  // q-points handled by this context: [q_begin, q_end) (a shard of the q loop; default all)
+  int q_begin = 0, q_end = -1;
+  // stored pairs delivered so far by the chunked device upload
+  int64_t pairs_set_gw = 0, pairs_set_hf = 0;
+  // statistics of the tensor-core contraction kernel (off unless requested)
+  bool stats_on = false;
+  std::vector<KernelRecord> records;
+  size_t records_used = 0;
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
 
   int64_t nao() const { return d.nao; }

@@ -139,7 +139,11 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
   };
 
   float t_p0 = 0, t_w = 0, t_sig = 0;
-  for (int q = 0; q < nk; ++q) {
+  // this context's share of the q loop (gw_cpu_kernel.cpp:45 distributes q over nodes the same way);
+  // the partial Sigma is already divided by nk, so shards sum to the full self-energy
+  const int q0 = std::max(0, c.q_begin);
+  const int q1 = c.q_end < 0 ? nk : std::min(nk, c.q_end);
+  for (int q = q0; q < q1; ++q) {
     // ---------------- polarization P0(tau, q), tau in the first half ---------
     GB_CUDA(cudaEventRecord(c.ev[1], st));
     GB_CUDA(cudaMemsetAsync(P0, 0, (size_t)nts * NQ * NQ * sizeof(cplx), st));

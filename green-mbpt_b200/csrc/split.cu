@@ -921,6 +921,19 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st) {
       int nsm = 148;
       GB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.device));
       const unsigned grid = (unsigned)std::min<int64_t>(ntiles, nsm);
+      KernelRecord* rec = nullptr;
+      if (c.stats_on) {
+        if (c.records_used == c.records.size()) {
+          KernelRecord r;
+          GB_CUDA(cudaEventCreate(&r.start));
+          GB_CUDA(cudaEventCreate(&r.stop));
+          c.records.push_back(r);
+        }
+        rec = &c.records[c.records_used++];
+        // FP64-equivalent work of this K chunk: 8 real flops per complex multiply-add
+        rec->alg_flops = 8.0 * (double)g0.M * (double)g0.N * (double)Kc * (double)nbatch;
+        GB_CUDA(cudaEventRecord(rec->start, st));
+      }
       switch (S) {
         case 2: split_gemm_tc_kernel<2><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
         case 3: split_gemm_tc_kernel<3><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
@@ -931,6 +944,7 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st) {
         default: split_gemm_tc_kernel<8><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
       }
       GB_CHECK_LAUNCH();
+      if (rec) GB_CUDA(cudaEventRecord(rec->stop, st));
     }
   }
 }

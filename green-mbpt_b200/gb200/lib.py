@@ -58,7 +58,8 @@ EXPORTED = [
     "gb200_set_kq_maps", "gb200_set_grid", "gb200_set_integrals", "gb200_set_precision", "gb200_gw_sigma",
     "gb200_gw_sigma_device", "gb200_hf_fock", "gb200_hf_fock_device", "gb200_dyson_set_hamiltonian",
     "gb200_dyson_find_mu", "gb200_dyson_compute_G", "gb200_dyson_electrons", "gb200_energy",
-    "gb200_iteration_device", "gb200_last_timings", "gb200_set_split_engine",
+    "gb200_iteration_device", "gb200_last_timings", "gb200_set_split_engine", "gb200_set_integrals_device",
+    "gb200_set_q_range", "gb200_dyson_solve_device", "gb200_energy_device", "gb200_stats_enable", "gb200_stats_read",
 ]
 
 
@@ -104,6 +105,13 @@ def load(path: str | None = None):
     L.gb200_iteration_device.argtypes = [vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, dp, dp, vp]
     L.gb200_last_timings.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     L.gb200_set_split_engine.argtypes = [vp, ip]
+    L.gb200_set_integrals_device.argtypes = [vp, ip, vp, ctypes.c_int64, ctypes.c_int64, vp]
+    L.gb200_set_q_range.argtypes = [vp, ip, ip]
+    L.gb200_dyson_solve_device.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_double, dp, vp, vp]
+    L.gb200_energy_device.argtypes = [vp, vp, vp, vp, dp, vp]
+    L.gb200_stats_enable.argtypes = [vp, ip]
+    ll = ctypes.POINTER(ctypes.c_longlong)
+    L.gb200_stats_read.argtypes = [vp, ll, ll, dp, dp]
     _lib = L
     return L
 
@@ -248,6 +256,38 @@ class Context:
                                                    float(tol), ctypes.byref(m), e if energies else None,
                                                    ctypes.c_void_p(stream)))
         return m.value, (tuple(e) if energies else None)
+
+    def set_integrals_device(self, V_ptr: int, pair_begin: int, pair_count: int, which=INTEGRALS_GW, stream: int = 0):
+        """Deliver stored pairs [pair_begin, pair_begin + pair_count) from device memory."""
+        self._check(self._L.gb200_set_integrals_device(self._h, which, ctypes.c_void_p(V_ptr), pair_begin, pair_count,
+                                                       ctypes.c_void_p(stream)))
+
+    def set_q_range(self, q_begin: int, q_end: int):
+        self._check(self._L.gb200_set_q_range(self._h, q_begin, q_end))
+
+    def dyson_solve_device(self, Sigma1_ptr, Sigma_ptr, nel, tol, mu, G_ptr, stream=0):
+        m = ctypes.c_double(mu)
+        self._check(self._L.gb200_dyson_solve_device(self._h, ctypes.c_void_p(Sigma1_ptr), ctypes.c_void_p(Sigma_ptr),
+                                                      float(nel), float(tol), ctypes.byref(m), ctypes.c_void_p(G_ptr),
+                                                      ctypes.c_void_p(stream)))
+        return m.value
+
+    def energy_device(self, G_ptr, Sigma1_ptr, Sigma_ptr, stream=0):
+        e = (ctypes.c_double * 3)()
+        self._check(self._L.gb200_energy_device(self._h, ctypes.c_void_p(G_ptr), ctypes.c_void_p(Sigma1_ptr),
+                                                ctypes.c_void_p(Sigma_ptr), e, ctypes.c_void_p(stream)))
+        return tuple(e)
+
+    def stats_enable(self, on=True):
+        self._check(self._L.gb200_stats_enable(self._h, 1 if on else 0))
+
+    def stats_read(self):
+        """(library launches so far, contraction-kernel launches, their device ms, their FP64-equivalent flops)."""
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        ms, fl = ctypes.c_double(), ctypes.c_double()
+        self._check(self._L.gb200_stats_read(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(ms),
+                                             ctypes.byref(fl)))
+        return a.value, b.value, ms.value, fl.value
 
     def last_timings(self):
         t = (ctypes.c_float * 4)()

@@ -102,7 +102,7 @@ class System:
 
 
 def make_system(mesh=(2, 2, 2), nao=10, naux=40, ns=1, beta=100.0, nts=60, nw=None, eps_range=2.0,
-                seed=0, madelung=0.0, grid: ChebyshevGrid | None = None) -> System:
+                seed=0, madelung=0.0, grid: ChebyshevGrid | None = None, with_integrals: bool = True) -> System:
     rng = np.random.default_rng(seed)
     nk = int(np.prod(mesh))
     grid = grid if grid is not None else cached_grid(float(beta), int(nts), nw, nw)
@@ -120,12 +120,22 @@ def make_system(mesh=(2, 2, 2), nao=10, naux=40, ns=1, beta=100.0, nts=60, nw=No
             G[:, s, k] = -np.einsum("ia,ta,ja->tij", U[s, k], f, np.conj(U[s, k]))
     npair = pair_count(nk)
     sd = 1.0 / np.sqrt(2.0 * naux)
-    V = (rng.standard_normal((npair, naux, nao, nao)) + 1j * rng.standard_normal((npair, naux, nao, nao))) * sd
-    for k in range(nk):
-        idx = k * (k + 1) // 2 + k
-        V[idx] = 0.5 * (V[idx] + np.conj(np.swapaxes(V[idx], -1, -2)))
+    if with_integrals:
+        V = (rng.standard_normal((npair, naux, nao, nao)) + 1j * rng.standard_normal((npair, naux, nao, nao))) * sd
+        for k in range(nk):
+            idx = k * (k + 1) // 2 + k
+            V[idx] = 0.5 * (V[idx] + np.conj(np.swapaxes(V[idx], -1, -2)))
+    else:
+        V = np.zeros((0, naux, nao, nao), dtype=np.complex128)
     return System(mesh=tuple(mesh), nk=nk, nao=nao, NQ=naux, ns=ns, beta=float(beta), grid=grid, eps=eps, U=U,
                   F=F, S=S, G=G, V_half=V, madelung=madelung, seed=seed)
+
+
+def random_pair(rng, naux, nao, hermitian=False):
+    """One V^Q_ij(k1,k2) block with the generator's distribution."""
+    sd = 1.0 / np.sqrt(2.0 * naux)
+    v = (rng.standard_normal((naux, nao, nao)) + 1j * rng.standard_normal((naux, nao, nao))) * sd
+    return 0.5 * (v + np.conj(np.swapaxes(v, -1, -2))) if hermitian else v
 
 
 def make_config(name: str, seed: int = 0, **over) -> System:
@@ -133,3 +143,38 @@ def make_config(name: str, seed: int = 0, **over) -> System:
     kw = dict(mesh=mesh, nao=nao, naux=naux, ns=ns, beta=beta, nts=nts, nw=nw, eps_range=er, seed=seed)
     kw.update(over)
     return make_system(**kw)
+
+
+def upload_device_integrals(ctx, nk: int, naux: int, nao: int, seed: int = 0, chunk_bytes: float = 2e9,
+                            device: int = 0):
+    """Generate V^Q_ij(k1,k2), k1 >= k2, on the GPU chunk by chunk and hand each chunk to the context.
+
+    Same distribution as make_system (complex Gaussian with E|V|^2 = 1/naux, Hermitian
+    diagonal pairs); the values come from torch's seeded CUDA generator, so they differ
+    from the host generator's.  Nothing of size nk(nk+1)/2 * naux * nao^2 is ever held
+    on the host or twice on the device.
+    """
+    import torch
+
+    npair = pair_count(nk)
+    pe = naux * nao * nao
+    per_chunk = max(1, int(chunk_bytes // (pe * 16)))
+    gen = torch.Generator(device=f"cuda:{device}")
+    gen.manual_seed(seed)
+    sd = 1.0 / np.sqrt(2.0 * naux)
+    diag = {k * (k + 1) // 2 + k for k in range(nk)}
+    for p0 in range(0, npair, per_chunk):
+        cnt = min(per_chunk, npair - p0)
+        re = torch.randn((cnt, naux, nao, nao), dtype=torch.float64, device=f"cuda:{device}", generator=gen)
+        im = torch.randn((cnt, naux, nao, nao), dtype=torch.float64, device=f"cuda:{device}", generator=gen)
+        v = torch.complex(re, im) * sd
+        del re, im
+        for p in range(p0, p0 + cnt):
+            if p in diag:
+                blk = v[p - p0]
+                v[p - p0] = 0.5 * (blk + blk.conj().transpose(-1, -2))
+        v = v.contiguous()
+        torch.cuda.synchronize(device)  # the context copies on its own stream
+        ctx.set_integrals_device(v.data_ptr(), p0, cnt)
+        torch.cuda.synchronize(device)
+        del v

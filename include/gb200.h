@@ -87,6 +87,19 @@ int gb200_set_grid(gb200_context* ctx, const double* Tnt_f, const double* Ttn_f,
  * (df_integral_t.h:64-92,162-177).  `which` = GB200_INTEGRALS_GW / _HF. */
 int gb200_set_integrals(gb200_context* ctx, int which, const double* V_half, int64_t npairs);
 
+/* The same integrals from device memory, in chunks: V_dev holds the stored pairs
+ * [pair_begin, pair_begin + pair_count) of the layout above.  A call with
+ * pair_begin = 0 starts a new set; the set is usable once every stored pair has
+ * been delivered.  `stream` is a cudaStream_t (or NULL for the context's stream). */
+int gb200_set_integrals_device(gb200_context* ctx, int which, const double* V_dev, int64_t pair_begin,
+                               int64_t pair_count, void* stream);
+
+/* Restrict the q loop to [q_begin, q_end): one shard of the reference's internode q
+ * distribution (gw_cpu_kernel.cpp:45-48).  Sigma then holds this shard's partial sum,
+ * already divided by nk, and the shards of all ranks add up to the full self-energy
+ * (the allreduce of :53-54).  Default: all q. */
+int gb200_set_q_range(gb200_context* ctx, int q_begin, int q_end);
+
 /* Contraction precision (GB200_PREC_*) and, for GB200_PREC_SPLIT, the number
  * of INT8 slices per operand (2..8). */
 int gb200_set_precision(gb200_context* ctx, int mode, int slices);
@@ -128,6 +141,23 @@ int gb200_energy(gb200_context* ctx, const double* G, const double* Sigma1, cons
 int gb200_iteration_device(gb200_context* ctx, double* G_dev, double* Sigma1_dev, double* Sigma_dev,
                            double madelung, double nel_target, double tol, double* mu_inout, double* e_out3,
                            void* stream);
+
+/* Dyson step on device buffers: find_mu (if nel_target > 0, dyson.cpp:101-174) then
+ * compute_G (dyson.cpp:238-288); Sigma1/Sigma are hermitized in place. */
+int gb200_dyson_solve_device(gb200_context* ctx, double* Sigma1_dev, double* Sigma_dev, double nel_target, double tol,
+                             double* mu_inout, double* G_dev, void* stream);
+/* compute_energy (common_utils.cpp:5-55) on device buffers. */
+int gb200_energy_device(gb200_context* ctx, const double* G_dev, const double* Sigma1_dev, const double* Sigma_dev,
+                        double* e_out3, void* stream);
+
+/* Kernel statistics for measurement: gb200_stats_enable(ctx, 1) starts timing every
+ * launch of the tensor-core contraction kernel with CUDA events on its stream;
+ * gb200_stats_read returns the library's total kernel-launch count (process wide),
+ * and for the contraction kernel its launches, summed device time (ms) and summed
+ * FP64-equivalent complex flops (8 per complex multiply-add). */
+int gb200_stats_enable(gb200_context* ctx, int on);
+int gb200_stats_read(gb200_context* ctx, long long* launches_total, long long* tc_launches, double* tc_ms,
+                     double* tc_alg_flops);
 
 /* Select the engine that multiplies the INT8 slice planes of GB200_PREC_SPLIT:
  * 0 = tcgen05 tensor cores (default), 1 = CUDA-core validation engine that

@@ -40,6 +40,7 @@ namespace {
 constexpr int KBLK = 64;          // bytes of K per pipeline stage (one 64B swizzle atom)
 constexpr int TILE_M = 128;       // real rows per CTA (64 complex rows)
 constexpr int EPI_CH = 32;        // result columns staged per epilogue step
+constexpr int EPI_LD = EPI_CH + 1; // staging row stride in complex values (one extra spreads the banks)
 constexpr int SMEM_BUDGET = 200 * 1024;
 constexpr int NWARPS = 10;        // producer, MMA, 8 epilogue warps
 constexpr int EPI_THREADS = 256;
@@ -211,9 +212,14 @@ struct SliceJob {
   int8_t* out;
   int32_t* expo;
   bool r_fast;                 // consecutive threads walk rows (else K) when reading
+  int single;                  // 1: the whole K range is one tile, exponents found in the same pass
 };
 
 constexpr int TR = 32, TK = 64, SL_NT = 256;
+// shared tile columns: one spare slot after every 8 complex values, so the 8 threads that
+// read consecutive groups of 8 columns of a row hit different banks
+constexpr int TKP = TK + TK / 8 + 1;
+__device__ __forceinline__ int tcol(int c) { return c + (c >> 3); }
 constexpr int EXP_EMPTY = -(1 << 30);
 
 __device__ __forceinline__ void enumerate_batch(const SliceJob& j, int64_t rb, int64_t& b0, int64_t& b1, int64_t& b2) {
@@ -227,7 +233,7 @@ __device__ __forceinline__ void enumerate_batch(const SliceJob& j, int64_t rb, i
 
 // Stage a TR x TK tile of the operand in shared memory (zero outside [0,R) x [0,K)).
 __device__ __forceinline__ void load_slice_tile(const SliceJob& j, const cplx* base, const int64_t* roff, int64_t r0,
-                                                int64_t kc, cplx (*tile)[TK + 1]) {
+                                                int64_t kc, cplx (*tile)[TKP]) {
   for (int e = threadIdx.x; e < TR * TK; e += SL_NT) {
     int rl, kl;
     if (j.r_fast) { rl = e % TR; kl = e / TR; } else { kl = e % TK; rl = e / TK; }
@@ -237,13 +243,13 @@ __device__ __forceinline__ void load_slice_tile(const SliceJob& j, const cplx* b
       v = base[roff[rl] + j.kmap(j.k0 + k)];
       if (j.conj) v.y = -v.y;
     }
-    tile[rl][kl] = v;
+    tile[rl][tcol(kl)] = v;
   }
 }
 
 // Pass 1: per-row exponent e (max |Re|,|Im| < 2^e) by atomicMax over K tiles.
 __global__ void __launch_bounds__(SL_NT) slice_expo_kernel(SliceJob j) {
-  __shared__ cplx tile[TR][TK + 1];
+  __shared__ cplx tile[TR][TKP];
   __shared__ int64_t roff[TR];
   const int64_t rb = blockIdx.z, r0 = (int64_t)blockIdx.x * TR, kc = (int64_t)blockIdx.y * TK;
   if (r0 >= j.R || kc >= j.K) return;
@@ -259,7 +265,7 @@ __global__ void __launch_bounds__(SL_NT) slice_expo_kernel(SliceJob j) {
   double m = 0.0;
 #pragma unroll
   for (int i = 0; i < TK / 8; ++i) {
-    cplx v = tile[rl][part * (TK / 8) + i];
+    cplx v = tile[rl][tcol(part * (TK / 8) + i)];
     m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
   }
   for (int o = 4; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -295,7 +301,7 @@ __device__ __forceinline__ uint32_t digit_byte(const Digits& d, int shift) {
 
 // Pass 2: slice planes, including the zero padding of rows and K.
 __global__ void __launch_bounds__(SL_NT) slice_write_kernel(SliceJob j) {
-  __shared__ cplx tile[TR][TK + 1];
+  __shared__ cplx tile[TR][TKP];
   __shared__ int64_t roff[TR];
   const int64_t rb = blockIdx.z, r0 = (int64_t)blockIdx.x * TR, kc = (int64_t)blockIdx.y * TK;
   int64_t b0, b1, b2;
@@ -308,12 +314,23 @@ __global__ void __launch_bounds__(SL_NT) slice_write_kernel(SliceJob j) {
   const int rl = threadIdx.x / 8, grp = threadIdx.x % 8;
   const int64_t r = r0 + rl;
   const int64_t k = kc + grp * 8;  // first of 8 complex K positions
-  if (r >= j.rpad || 2 * k >= j.kpad) return;
+  cplx vals[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) vals[i] = tile[rl][tcol(grp * 8 + i)];
   int e = 0;
-  if (r < j.R) {
+  if (j.single) {
+    // the 8 lanes of a row hold all of its K range: reduce the maximum here (before any lane leaves)
+    double m = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) m = fmax(m, fmax(fabs(vals[i].x), fabs(vals[i].y)));
+    for (int o = 4; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (m > 0.0) frexp(m, &e);
+    if (grp == 0 && r < j.R) j.expo[rb * j.e_ld + r] = e;
+  } else if (r < j.R) {
     e = j.expo[rb * j.e_ld + r];
     if (e == EXP_EMPTY) e = 0;
   }
+  if (r >= j.rpad || 2 * k >= j.kpad) return;
   const int S = j.S;
   // 2^(7S - e) in two exact power-of-two factors (the exponent can exceed the double range
   // for rows of tiny magnitude)
@@ -324,7 +341,7 @@ __global__ void __launch_bounds__(SL_NT) slice_write_kernel(SliceJob j) {
   Digits dr[8], di[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
-    const cplx v = tile[rl][grp * 8 + i];
+    const cplx v = vals[i];
     dr[i] = digits_of(v.x * sc1, sc2);
     di[i] = digits_of(v.y * sc1, sc2);
   }
@@ -412,7 +429,7 @@ __host__ __device__ inline SmemLayout smem_layout(int S, int BN, int stages) {
   L.stage_bytes = S * (L.a_plane_bytes + L.b_plane_bytes);
   L.stages = stages;
   L.ring_bytes = stages * L.stage_bytes;
-  L.ctile_bytes = (TILE_M / 2) * EPI_CH * 16;
+  L.ctile_bytes = ((TILE_M / 2) * EPI_LD * 16 + 1023) / 1024 * 1024;
   return L;
 }
 
@@ -643,7 +660,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             const double v = (S <= 5 ? (double)acc64[j] * pow2(-7 * (S + 1)) : accd[j]) * pow2(ea + sh_eB[c0 + cc + j]);
-            reinterpret_cast<double*>(&ctile[mloc * EPI_CH + cc + j])[r] = v;
+            reinterpret_cast<double*>(&ctile[mloc * EPI_LD + cc + j])[r] = v;
           }
         }
         const bool last = c0 + EPI_CH >= p.BN;
@@ -657,7 +674,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
           if (p.rows_fast) { ml = e % (TILE_M / 2); nl = e / (TILE_M / 2); } else { nl = e % cw; ml = e / cw; }
           if (ml >= mlim || c0 + nl >= nlim) continue;
           cplx* dst = Cb + sh_rowC[ml] + sh_colC[c0 + nl];
-          cplx val = cmul(p.alpha, ctile[ml * EPI_CH + nl]);
+          cplx val = cmul(p.alpha, ctile[ml * EPI_LD + nl]);
           if (has_beta) val = cadd(val, cmul(p.beta, *dst));
           *dst = val;
         }
@@ -805,6 +822,16 @@ unsigned blocks_for(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<
 // Slice one operand (rows x K) into planes + exponents.
 void run_slicer(SliceJob& j, int64_t nrb, cudaStream_t st) {
   const int64_t ne = nrb * j.e_ld;
+  require(nrb < 65536, GB200_ERR_INVALID, "split: too many operand batches");
+  if (j.kpad / 2 <= TK) {
+    // the whole contraction range fits one tile: one pass finds the exponents and writes the slices
+    j.single = 1;
+    dim3 g((unsigned)((j.rpad + TR - 1) / TR), 1, (unsigned)nrb);
+    slice_write_kernel<<<g, SL_NT, 0, st>>>(j);
+    GB_CHECK_LAUNCH();
+    return;
+  }
+  j.single = 0;
   fill_int_kernel<<<blocks_for(ne), 256, 0, st>>>(j.expo, ne, EXP_EMPTY);
   GB_CHECK_LAUNCH();
   require(nrb < 65536, GB200_ERR_INVALID, "split: too many operand batches");

@@ -108,6 +108,11 @@ struct HostIO {
 
 }  // namespace
 
+namespace gb200 {
+// message returned by gb200_last_error(NULL) for calls that have no context
+void set_thread_error(const std::string& msg) { g_create_error = msg; }
+}  // namespace gb200
+
 extern "C" {
 
 const char* gb200_version(void) { return "gb200 0.1.0 (integral format 1.0.0)"; }

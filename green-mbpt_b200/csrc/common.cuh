@@ -117,5 +117,6 @@ struct ZGemm {
 
 void zgemm_fp64(const ZGemm& g, cudaStream_t st);
 void validate(const ZGemm& g);
+void set_thread_error(const std::string& msg);
 
 }  // namespace gb200

@@ -60,6 +60,7 @@ EXPORTED = [
     "gb200_dyson_find_mu", "gb200_dyson_compute_G", "gb200_dyson_electrons", "gb200_energy",
     "gb200_iteration_device", "gb200_last_timings", "gb200_set_split_engine", "gb200_set_integrals_device",
     "gb200_set_q_range", "gb200_dyson_solve_device", "gb200_energy_device", "gb200_stats_enable", "gb200_stats_read",
+    "gb200_hf_fock_noalloc",
 ]
 
 
@@ -112,6 +113,7 @@ def load(path: str | None = None):
     L.gb200_stats_enable.argtypes = [vp, ip]
     ll = ctypes.POINTER(ctypes.c_longlong)
     L.gb200_stats_read.argtypes = [vp, ll, ll, dp, dp]
+    L.gb200_hf_fock_noalloc.argtypes = [ctypes.POINTER(Dims), vp, vp, vp, ctypes.c_double, vp, vp]
     _lib = L
     return L
 
@@ -297,6 +299,26 @@ class Context:
 
 def version():
     return load().gb200_version().decode()
+
+
+def hf_fock_noalloc(nk: int, nao: int, ns: int, NQ: int, V_ptr: int, dm_ptr: int, S_ptr: int, madelung: float,
+                    F_ptr: int, stream: int = 0):
+    """Fock matrix into F_ptr with no device allocation by the library (gb200_hf_fock_noalloc).
+
+    For callers that cannot allocate device memory while they run.  All
+    pointers are device addresses of complex128 arrays: V [nk][nk][NQ][nao][nao]
+    in full storage, dm, S, F [ns][nk][nao][nao].  The work is queued on
+    `stream` and runs asynchronously; calls that overlap on the GPU share one
+    fixed workspace and race.
+    """
+    L = load()
+    d = Dims(nk, nao, nao, ns, NQ, 0, 0, 0, 0.0)
+    rc = L.gb200_hf_fock_noalloc(ctypes.byref(d), ctypes.c_void_p(V_ptr), ctypes.c_void_p(dm_ptr),
+                                 ctypes.c_void_p(S_ptr), float(madelung), ctypes.c_void_p(F_ptr),
+                                 ctypes.c_void_p(stream))
+    if rc != OK:
+        msg = L.gb200_last_error(None).decode()
+        raise _EXC.get(rc, mbpt_kernel_error)(f"gb200_hf_fock_noalloc failed ({rc}): {msg}")
 
 
 def check_integral_version(v: str):

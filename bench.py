@@ -45,6 +45,7 @@ WORKLOADS = {
     "c2": "c2: nk=125 (5x5x5), nao=40, naux=250, ns=1, ntau=120, nw=120, beta=200, eps~U[-5,5]",
     "c1": "c1: nk=64 (4x4x4), nao=26, naux=150, ns=2, ntau=100, beta=100, eps~U[-2,2]",
     "c0": "c0: nk=8 (2x2x2), nao=10, naux=40, ns=1, ntau=60, beta=100, eps~U[-2,2]",
+    "c2k2": "c2k2: c2's shapes (nao=40, naux=250, ntau=120, nw=120) on a 2x1x1 mesh (nk=2): profiling case",
 }
 
 
@@ -186,7 +187,7 @@ def blas_threads():
 
 
 def setup_context(cfg, seed, slices, device, ws, rank):
-    from gb200 import lib, solvers, synth
+    from gb200 import lib, shard, solvers, synth
 
     s = synth.make_config(cfg, seed=seed, with_integrals=False)
     g = s.grid
@@ -198,8 +199,7 @@ def setup_context(cfg, seed, slices, device, ws, rank):
     ctx.set_hamiltonian(s.F, s.S)
     ctx.set_precision(lib.PREC_SPLIT, slices)
     if ws > 1:
-        per = (s.nk + ws - 1) // ws
-        ctx.set_q_range(min(s.nk, rank * per), min(s.nk, (rank + 1) * per))
+        ctx.set_q_range(*shard.q_shard(s.nk, ws, rank))
     return s, ctx
 
 
@@ -213,7 +213,7 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(minutes=15))
-    from gb200 import lib
+    from gb200 import lib, shard
 
     s, ctx = setup_context(args.config, args.seed, args.slices, local, ws, rank)
     dev = torch.device("cuda", local)
@@ -239,7 +239,7 @@ def run_ours(args):
         dm.copy_(G[-1] * (-1.0 if s.ns == 2 else -2.0))
         ctx.hf_fock_device(dm.data_ptr(), Sdev.data_ptr(), mad, S1.data_ptr(), stream=sptr)
         ctx.gw_sigma_device(G.data_ptr(), St.data_ptr(), stream=sptr)
-        dist.all_reduce(torch.view_as_real(St))
+        shard.reduce_partial_sigma(St, dist)
         state["mu"] = ctx.dyson_solve_device(S1.data_ptr(), St.data_ptr(), nel, tol, 0.0, G.data_ptr(), stream=sptr)
         state["E"] = ctx.energy_device(G.data_ptr(), S1.data_ptr(), St.data_ptr(), stream=sptr)
 
@@ -363,6 +363,32 @@ def main_ours(args):
     return line
 
 
+def main_gw_profile(args):
+    """--gw-q Q: only the GW self-energy over q-points [0, Q), W warm-up calls then K timed ones.
+
+    The kernel-profiling case (ncu captures of the contraction kernels): prints the
+    per-stage device times of the last call, not the headline metric.
+    """
+    import torch
+
+    torch.cuda.set_device(0)
+    s, ctx = setup_context(args.config, args.seed, args.slices, 0, 1, 0)
+    G = torch.from_numpy(s.G).cuda()
+    Sig = torch.empty_like(G)
+    ctx.set_q_range(0, min(args.gw_q, s.nk))
+    for _ in range(args.warmup):
+        ctx.gw_sigma_device(G.data_ptr(), Sig.data_ptr())
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(args.steps):
+        ctx.gw_sigma_device(G.data_ptr(), Sig.data_ptr())
+        out.append(ctx.last_timings())
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": WORKLOADS[args.config], "q_points": min(args.gw_q, s.nk),
+                      "precision": f"split, {args.slices} INT8 slices", "stage_ms": out[-1]}), flush=True)
+    ctx.close()
+
+
 def main_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -400,8 +426,10 @@ def parse(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--fp64-q", dest="fp64_q", type=int, default=1, help="q-points timed for the FP64 comparison")
     ap.add_argument("--no-fp64-sample", action="store_true")
+    ap.add_argument("--gw-q", dest="gw_q", type=int, default=0,
+                    help="profiling case: time only the GW self-energy over q-points [0, GW_Q)")
     a = ap.parse_args(argv)
-    if a.warmup < 3:
+    if a.warmup < 3 and not a.gw_q:
         ap.error("at least 3 warm-up steps")
     return a
 
@@ -410,5 +438,7 @@ if __name__ == "__main__":
     args = parse()
     if args.impl == "reference":
         main_reference(args)
+    elif args.gw_q:
+        main_gw_profile(args)
     else:
         main_ours(args)

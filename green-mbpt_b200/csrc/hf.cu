@@ -24,6 +24,25 @@ __global__ void dm_transpose_kernel(const cplx* dm, cplx* dmT, int ns, int nk, i
   }
 }
 
+// F[s][k0+kk][ij] += scale * sum_{k'} P[kk][s][k'][ij], summed in k' order
+__global__ void exchange_reduce_kernel(const cplx* P, cplx* F, int kbk, int ns, int nk, int k0, int64_t nao2,
+                                       double scale) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= (int64_t)kbk * ns * nao2) return;
+  const int64_t ij = e % nao2;
+  const int64_t ks = e / nao2;  // kk * ns + s
+  const int s = (int)(ks % ns), kk = (int)(ks / ns);
+  const cplx* p = P + ks * nk * nao2 + ij;
+  double re = 0.0, im = 0.0;
+  for (int kp = 0; kp < nk; ++kp) {
+    re += p[(int64_t)kp * nao2].x;
+    im += p[(int64_t)kp * nao2].y;
+  }
+  cplx* f = F + ((int64_t)s * nk + k0 + kk) * nao2 + ij;
+  f->x += scale * re;
+  f->y += scale * im;
+}
+
 ZOperand dense(const cplx* p, int64_t ld) {
   ZOperand o;
   o.ptr = p;
@@ -73,6 +92,10 @@ void hf_fock(Context& c, const cplx* dm, const cplx* S, double madelung, cplx* F
     zgemm_fp64(g, st);
   }
   // ---- exchange term, blocked over k ----
+  // Per k the exchange is an nao x nao result contracted over K = (k', Q, a), i.e. nk*NQ*nao
+  // terms.  One batch of the second contraction per (k, s, k') keeps the GPU busy (a single
+  // batch per k would leave most SMs idle); the per-k' partial results are then summed in k'
+  // order by exchange_reduce_kernel, so the result is deterministic.
   const int64_t per_k = (int64_t)ns * nk * pe;
   size_t free_b = 0, total_b = 0;
   GB_CUDA(cudaMemGetInfo(&free_b, &total_b));
@@ -80,6 +103,7 @@ void hf_fock(Context& c, const cplx* dm, const cplx* S, double madelung, cplx* F
   int kb = (int)std::max(1.0, std::floor(budget / ((double)per_k * sizeof(cplx))));
   kb = std::min(kb, nk);
   cplx* Y = (cplx*)c.scratch.get(SL_HF_Y, (size_t)kb * per_k * sizeof(cplx));
+  cplx* P = (cplx*)c.scratch.get(SL_TMP, (size_t)kb * ns * nk * nao2 * sizeof(cplx));
   for (int k0 = 0; k0 < nk; k0 += kb) {
     const int kbk = std::min(kb, nk - k0);
     ZGemm y;  // Y[kk][s][k'][(Q,i)][a] = sum_b V(k,k')[(Q,i)][b] dm[s][k'][b][a]
@@ -91,17 +115,20 @@ void hf_fock(Context& c, const cplx* dm, const cplx* S, double madelung, cplx* F
     y.C.ptr = Y; y.C.row = lin(nao); y.C.col = lin(1);
     y.C.bat.s0 = per_k; y.C.bat.s1 = (int64_t)nk * pe; y.C.bat.s2 = pe;
     zgemm_fp64(y, st);
-    ZGemm x;  // F[s][k][i][j] -= (c/nk) sum_{(k',Q),a} Y[kk][s][(k',Q)][i][a] conj(V(k,k')[(k',Q)][j][a])
-    x.M = nao; x.N = nao; x.K = (int64_t)nk * NQ * nao;
-    x.nb0 = kbk; x.nb2 = ns;
+    ZGemm x;  // P[kk][s][k'][i][j] = sum_{Q,a} Y[kk][s][k'][Q][i][a] conj(V(k,k')[Q][j][a])
+    x.M = nao; x.N = nao; x.K = (int64_t)NQ * nao;
+    x.nb0 = kbk; x.nb1 = ns; x.nb2 = nk;
     x.A.ptr = Y; x.A.row = lin(nao); x.A.col = two(nao, 1, nao2);
-    x.A.bat.s0 = per_k; x.A.bat.s2 = (int64_t)nk * pe;
+    x.A.bat.s0 = per_k; x.A.bat.s1 = (int64_t)nk * pe; x.A.bat.s2 = pe;
     x.B.ptr = V + (int64_t)k0 * nk * pe; x.B.row = two(nao, 1, nao2); x.B.col = lin(nao); x.B.conj = true;
-    x.B.bat.s0 = (int64_t)nk * pe;
-    x.C.ptr = F + (int64_t)k0 * nao2; x.C.row = lin(nao); x.C.col = lin(1);
-    x.C.bat.s0 = nao2; x.C.bat.s2 = (int64_t)nk * nao2;
-    x.alpha = cmk(-pref / nk, 0.0); x.beta = cmk(1.0, 0.0);
+    x.B.bat.s0 = (int64_t)nk * pe; x.B.bat.s2 = pe;
+    x.C.ptr = P; x.C.row = lin(nao); x.C.col = lin(1);
+    x.C.bat.s0 = (int64_t)ns * nk * nao2; x.C.bat.s1 = (int64_t)nk * nao2; x.C.bat.s2 = nao2;
     zgemm_fp64(x, st);
+    const int64_t nout = (int64_t)kbk * ns * nao2;
+    exchange_reduce_kernel<<<(unsigned)((nout + 255) / 256), 256, 0, st>>>(P, F, kbk, ns, nk, k0, nao2,
+                                                                          -pref / nk);
+    GB_CHECK_LAUNCH();
   }
   // ---- Madelung / Ewald term ----
   if (madelung != 0.0) {

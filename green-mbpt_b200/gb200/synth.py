@@ -29,6 +29,8 @@ CONFIGS = {
     "c1": ((4, 4, 4), 26, 150, 2, 100.0, 100, None, 2.0),
     "c2": ((5, 5, 5), 40, 250, 1, 200.0, 120, 120, 5.0),
     "c4": ((3, 3, 3), 20, 100, 1, 100.0, 80, None, 2.0),
+    # c2's orbital, auxiliary and time shapes on a 2x1x1 mesh: the kernel-profiling case
+    "c2k2": ((2, 1, 1), 40, 250, 1, 200.0, 120, 120, 5.0),
 }
 
 

@@ -231,34 +231,53 @@ __device__ __forceinline__ void enumerate_batch(const SliceJob& j, int64_t rb, i
   if (j.dep[0]) { b0 = r; }
 }
 
-// Stage a TR x TK tile of the operand in shared memory (zero outside [0,R) x [0,K)).
-__device__ __forceinline__ void load_slice_tile(const SliceJob& j, const cplx* base, const int64_t* roff, int64_t r0,
-                                                int64_t kc, cplx (*tile)[TKP]) {
-  for (int e = threadIdx.x; e < TR * TK; e += SL_NT) {
-    int rl, kl;
-    if (j.r_fast) { rl = e % TR; kl = e / TR; } else { kl = e % TK; rl = e / TK; }
-    const int64_t r = r0 + rl, k = kc + kl;
-    cplx v = cmk(0.0, 0.0);
-    if (r < j.R && k < j.K) {
-      v = base[roff[rl] + j.kmap(j.k0 + k)];
-      if (j.conj) v.y = -v.y;
+// Row and K offsets of a tile (one IdxMap evaluation per row and per K position instead of
+// one per element); callers synchronise before using them.
+__device__ __forceinline__ void tile_offsets(const SliceJob& j, int64_t r0, int64_t kc, int64_t* roff, int64_t* koff) {
+  const int t = threadIdx.x;
+  if (t < TR) roff[t] = (r0 + t < j.R) ? j.rmap(r0 + t) : 0;
+  else if (t >= 64 && t < 64 + TK) koff[t - 64] = (kc + t - 64 < j.K) ? j.kmap(j.k0 + kc + t - 64) : 0;
+}
+
+// Stage a TR x TK tile of the operand in shared memory (zero outside [0,R) x [0,K)); a thread
+// issues its loads four at a time before storing them.
+__device__ __forceinline__ void load_slice_tile(const SliceJob& j, const cplx* base, const int64_t* roff,
+                                                const int64_t* koff, int64_t r0, int64_t kc, cplx (*tile)[TKP]) {
+  constexpr int PER = TR * TK / SL_NT, BATCH = 4;
+#pragma unroll
+  for (int i0 = 0; i0 < PER; i0 += BATCH) {
+    cplx v[BATCH];
+#pragma unroll
+    for (int i = 0; i < BATCH; ++i) {
+      const int e = threadIdx.x + (i0 + i) * SL_NT;
+      int rl, kl;
+      if (j.r_fast) { rl = e % TR; kl = e / TR; } else { kl = e % TK; rl = e / TK; }
+      v[i] = cmk(0.0, 0.0);
+      if (r0 + rl < j.R && kc + kl < j.K) v[i] = __ldg(base + roff[rl] + koff[kl]);
     }
-    tile[rl][tcol(kl)] = v;
+#pragma unroll
+    for (int i = 0; i < BATCH; ++i) {
+      const int e = threadIdx.x + (i0 + i) * SL_NT;
+      int rl, kl;
+      if (j.r_fast) { rl = e % TR; kl = e / TR; } else { kl = e % TK; rl = e / TK; }
+      if (j.conj) v[i].y = -v[i].y;
+      tile[rl][tcol(kl)] = v[i];
+    }
   }
 }
 
 // Pass 1: per-row exponent e (max |Re|,|Im| < 2^e) by atomicMax over K tiles.
-__global__ void __launch_bounds__(SL_NT) slice_expo_kernel(SliceJob j) {
+__global__ void __launch_bounds__(SL_NT, 4) slice_expo_kernel(SliceJob j) {
   __shared__ cplx tile[TR][TKP];
-  __shared__ int64_t roff[TR];
+  __shared__ int64_t roff[TR], koff[TK];
   const int64_t rb = blockIdx.z, r0 = (int64_t)blockIdx.x * TR, kc = (int64_t)blockIdx.y * TK;
   if (r0 >= j.R || kc >= j.K) return;
   int64_t b0, b1, b2;
   enumerate_batch(j, rb, b0, b1, b2);
   const cplx* base = j.ptr + j.bat(b0, b1, b2);
-  if (threadIdx.x < TR) roff[threadIdx.x] = (r0 + threadIdx.x < j.R) ? j.rmap(r0 + threadIdx.x) : 0;
+  tile_offsets(j, r0, kc, roff, koff);
   __syncthreads();
-  load_slice_tile(j, base, roff, r0, kc, tile);
+  load_slice_tile(j, base, roff, koff, r0, kc, tile);
   __syncthreads();
   // 8 threads per row, 8 columns each
   const int rl = threadIdx.x / 8, part = threadIdx.x % 8;
@@ -292,24 +311,25 @@ __device__ __forceinline__ Digits digits_of(double a, double scale) {
   return d;
 }
 
-// signed digit s (top = 0) as a byte in the low 8 bits
-__device__ __forceinline__ uint32_t digit_byte(const Digits& d, int shift) {
-  uint32_t q = (uint32_t)(d.mag >> shift) & 127u;
-  q = (q ^ d.neg) - d.neg;  // conditional negate
+// signed digit (top = 0) of magnitude `mag` as a byte in the low 8 bits; bit 0 of `neg` is the sign
+__device__ __forceinline__ uint32_t digit_byte(uint64_t mag, uint32_t neg, int shift) {
+  const uint32_t m = 0u - (neg & 1u);  // 0 or 0xFFFFFFFF
+  uint32_t q = (uint32_t)(mag >> shift) & 127u;
+  q = (q ^ m) - m;  // conditional negate
   return q & 0xFFu;
 }
 
 // Pass 2: slice planes, including the zero padding of rows and K.
-__global__ void __launch_bounds__(SL_NT) slice_write_kernel(SliceJob j) {
+__global__ void __launch_bounds__(SL_NT, 4) slice_write_kernel(SliceJob j) {
   __shared__ cplx tile[TR][TKP];
-  __shared__ int64_t roff[TR];
+  __shared__ int64_t roff[TR], koff[TK];
   const int64_t rb = blockIdx.z, r0 = (int64_t)blockIdx.x * TR, kc = (int64_t)blockIdx.y * TK;
   int64_t b0, b1, b2;
   enumerate_batch(j, rb, b0, b1, b2);
   const cplx* base = j.ptr + j.bat(b0, b1, b2);
-  if (threadIdx.x < TR) roff[threadIdx.x] = (r0 + threadIdx.x < j.R) ? j.rmap(r0 + threadIdx.x) : 0;
+  tile_offsets(j, r0, kc, roff, koff);
   __syncthreads();
-  load_slice_tile(j, base, roff, r0, kc, tile);
+  load_slice_tile(j, base, roff, koff, r0, kc, tile);
   __syncthreads();
   const int rl = threadIdx.x / 8, grp = threadIdx.x % 8;
   const int64_t r = r0 + rl;
@@ -338,12 +358,17 @@ __global__ void __launch_bounds__(SL_NT) slice_write_kernel(SliceJob j) {
   const int ex1 = max(-1000, min(1000, ex));
   const double sc1 = __longlong_as_double((long long)(ex1 + 1023) << 52);
   const double sc2 = __longlong_as_double((long long)(max(-1022, min(1023, ex - ex1)) + 1023) << 52);
-  Digits dr[8], di[8];
+  // magnitudes of the truncated scaled values and their signs (one bit per real part)
+  uint64_t mr[8], mi[8];
+  uint32_t negs = 0;
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const cplx v = vals[i];
-    dr[i] = digits_of(v.x * sc1, sc2);
-    di[i] = digits_of(v.y * sc1, sc2);
+    const Digits a = digits_of(v.x * sc1, sc2), b = digits_of(v.y * sc1, sc2);
+    mr[i] = a.mag;
+    mi[i] = b.mag;
+    negs |= (a.neg & 1u) << (2 * i);
+    negs |= (b.neg & 1u) << (2 * i + 1);
   }
   const int64_t plane = j.rows_pad * j.kpad;
   int8_t* outb = j.out + rb * (int64_t)S * plane;
@@ -352,8 +377,10 @@ __global__ void __launch_bounds__(SL_NT) slice_write_kernel(SliceJob j) {
     uint32_t w0[4], w1[4];
 #pragma unroll
     for (int h = 0; h < 4; ++h) {
-      const uint32_t r0b = digit_byte(dr[2 * h], shift), i0b = digit_byte(di[2 * h], shift);
-      const uint32_t r1b = digit_byte(dr[2 * h + 1], shift), i1b = digit_byte(di[2 * h + 1], shift);
+      const uint32_t r0b = digit_byte(mr[2 * h], negs >> (4 * h), shift);
+      const uint32_t i0b = digit_byte(mi[2 * h], negs >> (4 * h + 1), shift);
+      const uint32_t r1b = digit_byte(mr[2 * h + 1], negs >> (4 * h + 2), shift);
+      const uint32_t i1b = digit_byte(mi[2 * h + 1], negs >> (4 * h + 3), shift);
       if (j.embed) {
         // row 2r: (re, -im) pairs; row 2r+1: (im, re) pairs
         const uint32_t ni0 = (0u - i0b) & 0xFFu, ni1 = (0u - i1b) & 0xFFu;

@@ -415,22 +415,27 @@ __device__ __forceinline__ double pow2(int e) {
   return __longlong_as_double((long long)(e + 1023) << 52);
 }
 
-// sum_d q_d 2^-7(d+2): exact in int64 while the digits cannot overflow it (S <= 5, |q_d| < 2^31),
-// then one rounding to double; FP64 accumulation in diagonal order beyond that.  Both engines
-// use this function, so they agree bit for bit.
+// int32 -> double on the FP64 pipe: the double with high word 0x43380000 and low word x + 2^31
+// is 1.5*2^52 + 2^31 + x exactly (IEEE-754 bit pattern), so one subtraction gives x.
+__device__ __forceinline__ double int_to_double(int32_t x) {
+  return __hiloint2double(0x43380000, (int)((uint32_t)x ^ 0x80000000u)) - 6755401588539392.0;
+}
+
+// Horner sum of the diagonals, sum_d q_d 128^(S-1-d), i.e. the value in units of
+// 2^(ea + eb - 7(S+1)).  With |q_d| < 2^31 the first four partial sums are exact (< 2^53), so
+// for S <= 5 the result is the exact sum rounded once.  The tensor-core epilogue evaluates the
+// same expression, so both engines agree bit for bit.
 __device__ __forceinline__ double combine_diagonals(const int32_t* q, int S) {
-  if (S <= 5) {
-    long long acc = 0;
-    for (int d = 0; d < S; ++d) acc += (long long)q[d] << (7 * (S - 1 - d));
-    return (double)acc * pow2(-7 * (S + 1));
-  }
-  double v = 0.0;
-  for (int d = 0; d < S; ++d) v = fma((double)q[d], pow2(-7 * (d + 2)), v);
+  double v = int_to_double(q[0]);
+  for (int d = 1; d < S; ++d) v = fma(v, 128.0, int_to_double(q[d]));
   return v;
 }
 
+// the factor of a result element: 2^ea (row) times 2^(eb - 7(S+1)) (column)
+__device__ __forceinline__ double result_scale(int ea, int eb, int S) { return pow2(ea) * pow2(eb - 7 * (S + 1)); }
+
 __device__ __forceinline__ void store_at(const GemmParams& p, cplx* dst, double re, double im, int ea, int eb) {
-  const double sc = pow2(ea + eb);
+  const double sc = result_scale(ea, eb, p.S);
   cplx v = cmul(p.alpha, cmk(re * sc, im * sc));
   if (p.beta.x != 0.0 || p.beta.y != 0.0) v = cadd(v, cmul(p.beta, *dst));
   *dst = v;
@@ -462,7 +467,7 @@ __host__ __device__ inline SmemLayout smem_layout(int S, int BN, int stages) {
 
 // bytes after the tile ring and the result tile: barriers, TMEM slot, flags, per-tile tables
 __host__ __device__ inline int misc_bytes(int stages, int BN) {
-  return (2 * stages + 4) * 8 + 16 + (TILE_M / 2 + BN) * 4 + (TILE_M / 2 + BN) * 8 + 64;
+  return (2 * stages + 4) * 8 + 16 + (TILE_M / 2 + BN) * 4 + (TILE_M / 2 + BN) * 8 + BN * 8 + 64;
 }
 
 struct TileCoord {
@@ -510,6 +515,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
   int32_t* sh_eB = sh_eA + TILE_M / 2;
   int64_t* sh_rowC = reinterpret_cast<int64_t*>(misc + 16 + ((TILE_M / 2 + p.BN) * 4 + 7) / 8 * 8);
   int64_t* sh_colC = sh_rowC + TILE_M / 2;
+  double* sh_csc = reinterpret_cast<double*>(sh_colC + p.BN);  // column factors 2^(eb - 7(S+1))
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   constexpr int S = SS;
@@ -633,6 +639,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
           const int64_t n = tc.ncol0 + (i - TILE_M / 2);
           sh_eB[i - TILE_M / 2] = n < p.N ? p.eB[tc.rbB * p.eB_ld + n] : 0;
           sh_colC[i - TILE_M / 2] = n < p.N ? p.C.col(n) : 0;
+          sh_csc[i - TILE_M / 2] = pow2(sh_eB[i - TILE_M / 2] - 7 * (S + 1));
         }
       }
       if (et == 0) {
@@ -649,7 +656,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
       tc_fence_after();
       const int mloc = row / 2;
       const int r = row & 1;
-      const int ea = sh_eA[mloc];
+      const double rs = pow2(sh_eA[mloc]);
       // a warp whose 32 rows are all padding skips the accumulator reads
       const bool live = tc.mrow0 + sp * 32 < 2 * p.M;
       const uint32_t acc = tmem_base + (uint32_t)buf * acc_cols + ((uint32_t)(sp * 32) << 16);
@@ -661,11 +668,11 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
         const int cc = half * 16;
         if (live && cc < cw) {
           // TMEM -> FP64 complex chunk: real rows write .x, imaginary rows .y.  The diagonals are
-          // combined exactly in int64 (S <= 5) or in FP64 in diagonal order, as combine_diagonals.
-          long long acc64[16];
+          // combined by Horner's rule in FP64 as in combine_diagonals (the first step from 0 is
+          // exact), then scaled by result_scale's two factors.
           double accd[16];
 #pragma unroll
-          for (int j = 0; j < 16; ++j) { acc64[j] = 0; accd[j] = 0.0; }
+          for (int j = 0; j < 16; ++j) accd[j] = 0.0;
 #pragma unroll
           for (int d0 = 0; d0 < S; d0 += 4) {
             int32_t q[4][16];
@@ -677,16 +684,13 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
             for (int dd = 0; dd < 4; ++dd) {
               if (d0 + dd < S) {
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                  if (S <= 5) acc64[j] += (long long)q[dd][j] << (7 * (S - 1 - (d0 + dd)));
-                  else accd[j] = fma((double)q[dd][j], pow2(-7 * (d0 + dd + 2)), accd[j]);
-                }
+                for (int j = 0; j < 16; ++j) accd[j] = fma(accd[j], 128.0, int_to_double(q[dd][j]));
               }
             }
           }
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
-            const double v = (S <= 5 ? (double)acc64[j] * pow2(-7 * (S + 1)) : accd[j]) * pow2(ea + sh_eB[c0 + cc + j]);
+            const double v = accd[j] * (rs * sh_csc[c0 + cc + j]);
             reinterpret_cast<double*>(&ctile[mloc * EPI_LD + cc + j])[r] = v;
           }
         }
@@ -695,15 +699,28 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
         asm volatile("bar.sync 1, 256;" ::: "memory");
         if (last && et == 0) mbar_arrive_local(&acce_bar[buf]);  // this accumulator set may be reused
         // coalesced write-out: consecutive threads walk the result index with unit stride
+        // (four elements per round, their loads ahead of their stores)
         const int total = (TILE_M / 2) * cw;
-        for (int e = et; e < total; e += EPI_THREADS) {
-          int ml, nl;
-          if (p.rows_fast) { ml = e % (TILE_M / 2); nl = e / (TILE_M / 2); } else { nl = e % cw; ml = e / cw; }
-          if (ml >= mlim || c0 + nl >= nlim) continue;
-          cplx* dst = Cb + sh_rowC[ml] + sh_colC[c0 + nl];
-          cplx val = cmul(p.alpha, ctile[ml * EPI_LD + nl]);
-          if (has_beta) val = cadd(val, cmul(p.beta, *dst));
-          *dst = val;
+        for (int e0 = et; e0 < total; e0 += 4 * EPI_THREADS) {
+          cplx v[4];
+          cplx* d[4];
+          bool ok[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int e = e0 + u * EPI_THREADS;
+            int ml, nl;
+            if (p.rows_fast) { ml = e % (TILE_M / 2); nl = e / (TILE_M / 2); } else { nl = e % cw; ml = e / cw; }
+            ok[u] = e < total && ml < mlim && c0 + nl < nlim;
+            d[u] = ok[u] ? Cb + sh_rowC[ml] + sh_colC[c0 + nl] : nullptr;
+            v[u] = ok[u] ? ctile[ml * EPI_LD + nl] : cmk(0.0, 0.0);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (!ok[u]) continue;
+            cplx val = cmul(p.alpha, v[u]);
+            if (has_beta) val = cadd(val, cmul(p.beta, *d[u]));
+            *d[u] = val;
+          }
         }
         asm volatile("bar.sync 1, 256;" ::: "memory");
       }
@@ -881,11 +898,11 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st) {
   const int S = c.slices;
   require(S >= 2 && S <= 8, GB200_ERR_INVALID, "split: slices out of range");
   require(g0.K > 0, GB200_ERR_INVALID, "split: empty contraction");
-  // Short contractions (a few K blocks per tile) are epilogue-bound: two TMEM accumulator sets of
-  // S * BN <= 256 columns let the epilogue of one tile overlap the MMAs of the next.  Long
-  // contractions are MMA-bound: one set of up to 512 columns and wider tiles.
-  const bool short_k = rup(2 * std::min<int64_t>(g0.K, 1 << 20), KBLK) / KBLK <= 8;
-  const int nbuf = short_k ? 2 : 1;
+  // One TMEM accumulator set of up to 512 columns and the widest tile it allows: the cost per
+  // tile is largely fixed (tables, barriers, TMEM round trips), and halving the tile width to
+  // double-buffer the accumulators (so that the epilogue overlaps the next tile's MMAs) measured
+  // 20-27% slower for the short contractions on B200.
+  const int nbuf = 1;
   const int BN = std::min<int>(max_bn(S, 512 / nbuf), (int)rup(g0.N, 16));
   // largest K chunk for which no INT32 diagonal can overflow: S * 2K * 127^2 < 2^31
   int64_t kmax = (int64_t)(2147483647.0 / (2.0 * 127.0 * 127.0 * S));

@@ -73,8 +73,16 @@ struct IdxMap {
 
   __host__ __device__ __forceinline__ int64_t operator()(int64_t i) const {
     if (n_in == 0) return i * s_in;
-    int64_t o = i / n_in;
-    int64_t r = i - o * n_in;
+    int64_t o, r;
+    if (((uint64_t)i | (uint64_t)n_in) < 0x80000000ull) {
+      // 32-bit division: several times cheaper than the 64-bit one on the GPU
+      const uint32_t q = (uint32_t)i / (uint32_t)n_in;
+      o = q;
+      r = (int64_t)((uint32_t)i - q * (uint32_t)n_in);
+    } else {
+      o = i / n_in;
+      r = i - o * n_in;
+    }
     return (tab ? tab[o] : o * s_out) + r * s_in;
   }
 };

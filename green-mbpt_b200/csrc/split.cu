@@ -475,18 +475,22 @@ struct TileCoord {
 };
 
 __device__ __forceinline__ TileCoord tile_coord(const GemmParams& p, int64_t t) {
+  // tile and batch counts fit 32 bits (the host checks), so the divisions are 32-bit
   TileCoord c;
-  const int64_t per_batch = (int64_t)p.tiles_m * p.tiles_n;
-  const int64_t bz = t / per_batch;
-  const int64_t rem = t - bz * per_batch;
-  const int64_t by = rem / p.tiles_n, bx = rem - by * p.tiles_n;  // N fastest: neighbours share A
-  c.b2 = bz % p.nb2;
-  c.b1 = (bz / p.nb2) % p.nb1;
-  c.b0 = bz / (p.nb2 * p.nb1);
+  const uint32_t per_batch = (uint32_t)p.tiles_m * (uint32_t)p.tiles_n;
+  const uint32_t t32 = (uint32_t)t;
+  const uint32_t bz = t32 / per_batch;
+  const uint32_t rem = t32 - bz * per_batch;
+  const uint32_t by = rem / (uint32_t)p.tiles_n, bx = rem - by * (uint32_t)p.tiles_n;  // N fastest: neighbours share A
+  const uint32_t nb2 = (uint32_t)p.nb2, nb1 = (uint32_t)p.nb1;
+  const uint32_t bq = bz / nb2;
+  c.b2 = bz - bq * nb2;
+  c.b1 = bq % nb1;
+  c.b0 = bq / nb1;
   c.rbA = reduced_batch(p.depA, c.b0, c.b1, c.b2, p.nb1, p.nb2);
   c.rbB = reduced_batch(p.depB, c.b0, c.b1, c.b2, p.nb1, p.nb2);
-  c.mrow0 = by * TILE_M;
-  c.ncol0 = bx * p.BN;
+  c.mrow0 = (int64_t)by * TILE_M;
+  c.ncol0 = (int64_t)bx * p.BN;
   return c;
 }
 
@@ -673,15 +677,17 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
           double accd[16];
 #pragma unroll
           for (int j = 0; j < 16; ++j) accd[j] = 0.0;
+          // up to six diagonals per TMEM round trip (all of them for S <= 6)
+          constexpr int DB = S <= 6 ? S : 4;
 #pragma unroll
-          for (int d0 = 0; d0 < S; d0 += 4) {
-            int32_t q[4][16];
+          for (int d0 = 0; d0 < S; d0 += DB) {
+            int32_t q[DB][16];
 #pragma unroll
-            for (int dd = 0; dd < 4; ++dd)
+            for (int dd = 0; dd < DB; ++dd)
               if (d0 + dd < S) tmem_ld16(acc + (uint32_t)((d0 + dd) * p.BN + c0 + cc), q[dd]);
             tmem_wait_ld();
 #pragma unroll
-            for (int dd = 0; dd < 4; ++dd) {
+            for (int dd = 0; dd < DB; ++dd) {
               if (d0 + dd < S) {
 #pragma unroll
                 for (int j = 0; j < 16; ++j) accd[j] = fma(accd[j], 128.0, int_to_double(q[dd][j]));
@@ -989,6 +995,7 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st) {
       require(smem <= 227 * 1024, GB200_ERR_INVALID, "split: shared memory budget exceeded");
       // persistent launch: one CTA per SM walks the tiles
       const int64_t ntiles = (int64_t)p.tiles_m * p.tiles_n * nbatch;
+      require(ntiles < (1LL << 31), GB200_ERR_INVALID, "split: too many tiles for one launch");
       int nsm = 148;
       GB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.device));
       const unsigned grid = (unsigned)std::min<int64_t>(ntiles, nsm);

@@ -28,6 +28,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 
@@ -181,6 +182,7 @@ struct GemmParams {
   int64_t eA_ld, eB_ld;
   ZResult C;
   cplx alpha, beta;
+  int alpha_pow2;  // alpha is real and a power of two (possibly negative)
   int* err;
 };
 
@@ -319,37 +321,10 @@ __device__ __forceinline__ uint32_t digit_byte(uint64_t mag, uint32_t neg, int s
   return q & 0xFFu;
 }
 
-// Pass 2: slice planes, including the zero padding of rows and K.
-__global__ void __launch_bounds__(SL_NT, 4) slice_write_kernel(SliceJob j) {
-  __shared__ cplx tile[TR][TKP];
-  __shared__ int64_t roff[TR], koff[TK];
-  const int64_t rb = blockIdx.z, r0 = (int64_t)blockIdx.x * TR, kc = (int64_t)blockIdx.y * TK;
-  int64_t b0, b1, b2;
-  enumerate_batch(j, rb, b0, b1, b2);
-  const cplx* base = j.ptr + j.bat(b0, b1, b2);
-  tile_offsets(j, r0, kc, roff, koff);
-  __syncthreads();
-  load_slice_tile(j, base, roff, koff, r0, kc, tile);
-  __syncthreads();
-  const int rl = threadIdx.x / 8, grp = threadIdx.x % 8;
-  const int64_t r = r0 + rl;
-  const int64_t k = kc + grp * 8;  // first of 8 complex K positions
-  cplx vals[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) vals[i] = tile[rl][tcol(grp * 8 + i)];
-  int e = 0;
-  if (j.single) {
-    // the 8 lanes of a row hold all of its K range: reduce the maximum here (before any lane leaves)
-    double m = 0.0;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) m = fmax(m, fmax(fabs(vals[i].x), fabs(vals[i].y)));
-    for (int o = 4; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (m > 0.0) frexp(m, &e);
-    if (grp == 0 && r < j.R) j.expo[rb * j.e_ld + r] = e;
-  } else if (r < j.R) {
-    e = j.expo[rb * j.e_ld + r];
-    if (e == EXP_EMPTY) e = 0;
-  }
+// Write the S digit planes of 8 consecutive K positions (from k) of row r with row exponent e,
+// including the zero padding of rows and K.
+__device__ __forceinline__ void write_digits(const SliceJob& j, const cplx (&vals)[8], int64_t rb, int64_t r, int64_t k,
+                                             int e) {
   if (r >= j.rpad || 2 * k >= j.kpad) return;
   const int S = j.S;
   // 2^(7S - e) in two exact power-of-two factors (the exponent can exceed the double range
@@ -397,6 +372,87 @@ __global__ void __launch_bounds__(SL_NT, 4) slice_write_kernel(SliceJob j) {
     } else {
       *reinterpret_cast<uint4*>(p + r * j.kpad + 2 * k) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
     }
+  }
+}
+
+// Pass 2: slice planes, including the zero padding of rows and K.
+__global__ void __launch_bounds__(SL_NT, 4) slice_write_kernel(SliceJob j) {
+  __shared__ cplx tile[TR][TKP];
+  __shared__ int64_t roff[TR], koff[TK];
+  const int64_t rb = blockIdx.z, r0 = (int64_t)blockIdx.x * TR, kc = (int64_t)blockIdx.y * TK;
+  int64_t b0, b1, b2;
+  enumerate_batch(j, rb, b0, b1, b2);
+  const cplx* base = j.ptr + j.bat(b0, b1, b2);
+  tile_offsets(j, r0, kc, roff, koff);
+  __syncthreads();
+  load_slice_tile(j, base, roff, koff, r0, kc, tile);
+  __syncthreads();
+  const int rl = threadIdx.x / 8, grp = threadIdx.x % 8;
+  const int64_t r = r0 + rl;
+  const int64_t k = kc + grp * 8;  // first of 8 complex K positions
+  cplx vals[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) vals[i] = tile[rl][tcol(grp * 8 + i)];
+  int e = 0;
+  if (j.single) {
+    // the 8 lanes of a row hold all of its K range: reduce the maximum here (before any lane leaves)
+    double m = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) m = fmax(m, fmax(fabs(vals[i].x), fabs(vals[i].y)));
+    for (int o = 4; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (m > 0.0) frexp(m, &e);
+    if (grp == 0 && r < j.R) j.expo[rb * j.e_ld + r] = e;
+  } else if (r < j.R) {
+    e = j.expo[rb * j.e_ld + r];
+    if (e == EXP_EMPTY) e = 0;
+  }
+  write_digits(j, vals, rb, r, k, e);
+}
+
+// Both passes in one block for contractions of moderate length: a block owns TR rows over the
+// whole contraction range, finds their exponents, then reads the rows again (from L2) and writes
+// the slices.  The operand makes one trip from HBM instead of two.
+__global__ void __launch_bounds__(SL_NT, 3) slice_fused_kernel(SliceJob j, int nkt) {
+  __shared__ cplx tile[TR][TKP];
+  __shared__ int64_t roff[TR], koff[TK];
+  __shared__ double rmax[TR];
+  const int64_t rb = blockIdx.z, r0 = (int64_t)blockIdx.x * TR;
+  int64_t b0, b1, b2;
+  enumerate_batch(j, rb, b0, b1, b2);
+  const cplx* base = j.ptr + j.bat(b0, b1, b2);
+  const int rl = threadIdx.x / 8, grp = threadIdx.x % 8;
+  if (threadIdx.x < TR) rmax[threadIdx.x] = 0.0;
+  for (int kt = 0; kt < nkt; ++kt) {
+    const int64_t kc = (int64_t)kt * TK;
+    tile_offsets(j, r0, kc, roff, koff);
+    __syncthreads();
+    load_slice_tile(j, base, roff, koff, r0, kc, tile);
+    __syncthreads();
+    double m = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const cplx v = tile[rl][tcol(grp * 8 + i)];
+      m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+    }
+    for (int o = 4; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (grp == 0) rmax[rl] = fmax(rmax[rl], m);
+    __syncthreads();
+  }
+  const int64_t r = r0 + rl;
+  int e = 0;
+  if (rmax[rl] > 0.0) frexp(rmax[rl], &e);
+  if (grp == 0 && r < j.R) j.expo[rb * j.e_ld + r] = e;
+  for (int kt = 0; kt < nkt; ++kt) {
+    const int64_t kc = (int64_t)kt * TK;
+    tile_offsets(j, r0, kc, roff, koff);
+    __syncthreads();
+    load_slice_tile(j, base, roff, koff, r0, kc, tile);
+    __syncthreads();
+    cplx vals[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) vals[i] = tile[rl][tcol(grp * 8 + i)];
+    __syncthreads();  // the next tile overwrites `tile`
+    write_digits(j, vals, rb, r, kc + grp * 8, e);
   }
 }
 
@@ -660,7 +716,10 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
       tc_fence_after();
       const int mloc = row / 2;
       const int r = row & 1;
-      const double rs = pow2(sh_eA[mloc]);
+      // a real alpha that is a power of two is folded into the row factor (exact, so the result
+      // equals the validation engine's alpha * value); the write-out is then a plain copy
+      const bool alpha_in_tile = p.alpha_pow2 != 0;
+      const double rs = alpha_in_tile ? pow2(sh_eA[mloc]) * p.alpha.x : pow2(sh_eA[mloc]);
       // a warp whose 32 rows are all padding skips the accumulator reads
       const bool live = tc.mrow0 + sp * 32 < 2 * p.M;
       const uint32_t acc = tmem_base + (uint32_t)buf * acc_cols + ((uint32_t)(sp * 32) << 16);
@@ -723,7 +782,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             if (!ok[u]) continue;
-            cplx val = cmul(p.alpha, v[u]);
+            cplx val = alpha_in_tile ? v[u] : cmul(p.alpha, v[u]);
             if (has_beta) val = cadd(val, cmul(p.beta, *d[u]));
             *d[u] = val;
           }
@@ -882,6 +941,14 @@ void run_slicer(SliceJob& j, int64_t nrb, cudaStream_t st) {
     return;
   }
   j.single = 0;
+  const int64_t nkt = (j.kpad / 2 + TK - 1) / TK;  // K tiles covering the padded range
+  if (nkt <= 8) {
+    // moderate contraction length: one block per TR rows does both passes
+    dim3 g((unsigned)((j.rpad + TR - 1) / TR), 1, (unsigned)nrb);
+    slice_fused_kernel<<<g, SL_NT, 0, st>>>(j, (int)nkt);
+    GB_CHECK_LAUNCH();
+    return;
+  }
   fill_int_kernel<<<blocks_for(ne), 256, 0, st>>>(j.expo, ne, EXP_EMPTY);
   GB_CHECK_LAUNCH();
   require(nrb < 65536, GB200_ERR_INVALID, "split: too many operand batches");
@@ -960,6 +1027,10 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st) {
     p.eA = se.expA.p; p.eB = se.expB.p; p.eA_ld = rowsA_pad / 2; p.eB_ld = rowsB_pad;
     p.C = g0.C; p.alpha = g0.alpha; p.beta = (k0 == 0) ? g0.beta : cmk(1.0, 0.0);
     p.err = se.err.p;
+    {
+      int aexp = 0;
+      p.alpha_pow2 = (g0.alpha.y == 0.0 && g0.alpha.x != 0.0 && std::fabs(std::frexp(g0.alpha.x, &aexp)) == 0.5) ? 1 : 0;
+    }
     p.rows_fast = std::abs(g0.C.row.s_in) < std::abs(g0.C.col.s_in) ? 1 : 0;
     const int64_t nbatch = g0.nb0 * g0.nb1 * g0.nb2;
     require(nbatch < 65536, GB200_ERR_INVALID, "split: too many batches for one launch");

@@ -40,6 +40,11 @@ sys.path.insert(0, os.path.join(ROOT, "green-mbpt_b200"))
 import numpy as np  # noqa: E402
 
 METRIC = "GW iterations/s at nk=125,nao=40: split-prec vs FP64 on B200, max|ΔΣ|≤1e-8"
+# DRAM bytes (read + write) per FP64-equivalent flop of the tensor-core contraction kernel, from
+# one ncu capture of its six launch shapes on the c2-shaped profiling case (c2k2): 8.18 GB for
+# 3.80e11 flops.  Each shape's traffic scales with its k-point batch as its flops do, so the
+# roofline traffic per launch is this ratio times the step's flops per launch.
+TC_DRAM_BYTES_PER_FLOP = 8.18e9 / 3.80e11
 UNIT = "iterations/s"
 WORKLOADS = {
     "c2": "c2: nk=125 (5x5x5), nao=40, naux=250, ns=1, ntau=120, nw=120, beta=200, eps~U[-5,5]",
@@ -267,9 +272,11 @@ def run_ours(args):
     ctx.stats_enable(True)
     launches0 = ctx.stats_read()[0]
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    torch.cuda.profiler.start()  # a profiler started with capture off records the timed steps only
     for k in range(args.steps):
         step(evs[k])
     torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -339,7 +346,9 @@ def main_ours(args):
                        "parallelism": f"q-sharded over {ws} GPU(s), NCCL all-reduce of Sigma" if ws > 1 else "1 GPU",
                        "l2": "inputs larger than L2 (G 384 MB, V 100 GB): no flush"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": bf16_peak, "unit": "TFLOP/s",
-                         "frac": (achieved / bf16_peak) if achieved else None, "traffic": None,
+                         "frac": (achieved / bf16_peak) if achieved else None,
+                         "traffic": (TC_DRAM_BYTES_PER_FLOP * r["tc_fl"] / r["tc_n"]) if r["tc_n"] else None,
+                         "traffic_unit": "bytes per launch (scaled from the c2k2 ncu capture)",
                          "kernel": "split_gemm_tc_kernel (tcgen05 kind::i8)", "launches": r["tc_n"],
                          "peak_source": f"{peak_src} bf16 dense sustained; achieved counts FP64-equivalent complex flops"},
             "cpu_baseline": {"value": 1.0 / cpu_est, "unit": UNIT, "cores": blas_threads(), "kind": "port",
@@ -380,10 +389,12 @@ def main_gw_profile(args):
         ctx.gw_sigma_device(G.data_ptr(), Sig.data_ptr())
     torch.cuda.synchronize()
     out = []
+    torch.cuda.profiler.start()  # a profiler started with capture off records the timed calls only
     for _ in range(args.steps):
         ctx.gw_sigma_device(G.data_ptr(), Sig.data_ptr())
         out.append(ctx.last_timings())
     torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     print(json.dumps({"profile_case": WORKLOADS[args.config], "q_points": min(args.gw_q, s.nk),
                       "precision": f"split, {args.slices} INT8 slices", "stage_ms": out[-1]}), flush=True)
     ctx.close()

@@ -1,12 +1,12 @@
 """Minimal read-only HDF5 reader (pure Python + numpy + zlib).
 
-It covers exactly what the green-mbpt test fixtures use: superblock v0/v1,
+It covers what green-mbpt's input and integral files use: superblock v0/v1,
 version-1 object headers with continuation blocks, old-style groups
 (symbol-table message -> v1 group B-tree -> SNOD nodes + local heap),
 contiguous / compact / chunked (v1 chunk B-tree) layouts, the deflate and
 shuffle filters, fixed-point, floating-point and string datatypes, and
-attributes.  It exists only to turn the reference's HDF5 fixtures into small
-numpy golden files; it is test infrastructure, not part of the library.
+attributes.  There is no h5py or libhdf5 in this environment; gb200.inputs
+reads the solver's input files with it.
 
 The format facts used here follow the public HDF5 File Format Specification
 (version 3.0), sections II (superblock), III.A/B (B-trees, symbol table

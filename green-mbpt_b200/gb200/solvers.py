@@ -47,6 +47,48 @@ def make_context(system: System, device: int = 0, precision: int = lib.PREC_FP64
     return ctx
 
 
+def context_from_files(input_path: str, hf_integrals: str | None = None, gw_integrals: str | None = None,
+                       grid=None, beta: float | None = None, device: int = 0):
+    """A context for a system written in green-mbpt's file format.
+
+    input_path: input.h5 (parameters, Hamiltonian blocks, k-point symmetry); hf_integrals /
+    gw_integrals: the integral directories (meta.h5 + VQ_<c>.h5) of the HF and GW kernels.
+    Objects at irreducible k-points and irreducible k-pair integrals are expanded to the full
+    zone on the host (inputs.KSymmetry).  `grid` (a grids.ChebyshevGrid or any object with
+    Tnt_f, Ttn_f, Tnt_b, Ttn_b, wsample_f, nts, nw, nw_b) is needed for GW and the Dyson step.
+    Returns (context, input dictionary).
+    """
+    from . import inputs
+    inp = inputs.read_input(input_path)
+    sym = inp["symmetry"]
+    nk, nao, nso, ns, NQ = inp["nk"], inp["nao"], inp["nso"], inp["ns"], inp["NQ"]
+    if nso != nao:
+        raise lib.mbpt_kernel_error("two-component (X2C) inputs are not supported by the GPU kernels")
+    if grid is not None:
+        ctx = lib.Context(nk, nao, ns, NQ, grid.nts, grid.nw, grid.nw_b, float(beta if beta is not None else grid.beta),
+                          device=device)
+        ctx.set_grid(grid.Tnt_f, grid.Ttn_f, grid.Tnt_b, grid.Ttn_b, grid.wsample_f)
+    else:
+        ctx = lib.Context(nk, nao, ns, NQ, 2, 2, 3, float(beta or 1.0), device=device)
+    if inp.get("k_frac") is not None:
+        kp, km = inputs.kq_maps_from_points(inp["k_frac"])
+        ctx.set_kq_maps(kp, km)
+    npairs = len(sym.kpair_irre)
+    if hf_integrals:
+        store, _ = inputs.read_integrals(hf_integrals, npairs)
+        ctx.set_integrals(sym.half_storage(store), lib.INTEGRALS_HF)
+    if gw_integrals:
+        store, _ = inputs.read_integrals(gw_integrals, npairs)
+        ctx.set_integrals(sym.half_storage(store), lib.INTEGRALS_GW)
+    if "S_ibz" in inp:
+        inp["S"] = sym.full_from_ibz(inp["S_ibz"])
+    if "H_ibz" in inp:
+        inp["H"] = sym.full_from_ibz(inp["H_ibz"])
+        if "S" in inp:
+            ctx.set_hamiltonian(inp["H"], inp["S"])
+    return ctx, inp
+
+
 class gw_solver:
     """GW self-energy through the B200 kernel (custom_gw_kernel callback)."""
 

@@ -6,7 +6,7 @@ this repository:
     python tests/golden/make_golden.py /path/to/green-mbpt
 
 It reads test/data/{HF,HF_X2C}/{input.h5,data.h5,df_hf_int/*} of the
-reference with the minimal HDF5 reader in h5lite.py and writes
+reference with the minimal HDF5 reader gb200.h5lite and writes
 tests/golden/{hf,hf_x2c}.npz holding exactly what one call of the reference's
 ``solve_hf`` test (test/solvers_test.cpp:27-78) consumes and produces:
 G(tau = beta) (the last tau slice of ``G_tau``), the irreducible k-pair chunk of
@@ -24,8 +24,8 @@ import sys
 
 import numpy as np
 
-sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
-from h5lite import H5File  # noqa: E402
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "..", "green-mbpt_b200"))
+from gb200.h5lite import H5File  # noqa: E402
 
 
 def _cplx(a):

@@ -45,22 +45,21 @@ def test_hf_parity(gpu, name):
 
 
 def test_hf_golden_through_gpu(gpu):
-    """The reference's HF fixture (k-point symmetry expanded on the host) through the GPU kernel."""
+    """The reference's HF fixture through the GPU kernel, the k-point symmetry expanded by the
+    library's own host code (gb200.inputs.KSymmetry), compared with the reference's Sigma1."""
+    from gb200 import inputs
     d = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "hf.npz")))
-    sym = O.RefSymmetry(d["bz2ibz"], d["ibz2bz"], d["tr_conj"], d["k_sym_transform_ao"], d["conj_pairs_list"],
-                        d["trans_pairs_list"], d["kpair_irre_list"], d["weight_ibz"])
+    sym = inputs.KSymmetry(d["bz2ibz"], d["ibz2bz"], d["tr_conj"], d["k_sym_transform_ao"], d["conj_pairs_list"],
+                           d["trans_pairs_list"], d["kpair_irre_list"], d["weight_ibz"])
     ns, nk, nao, NQ = int(d["ns"]), int(d["nk"]), int(d["nao"]), int(d["NQ"])
-    dm_ibz = O.hf_density(d["G_beta"][None], ns)
-    dm = np.stack([np.stack([sym.value_AO(dm_ibz[s], k) for k in range(nk)]) for s in range(ns)])
-    S = np.stack([np.stack([sym.value_AO(d["S_ibz"][s], k) for k in range(nk)]) for s in range(ns)])
-    for s in range(ns):
-        for ik, k in enumerate(sym.ibz2bz):
-            S[s, k] = d["S_ibz"][s, ik]
-    Vh = np.stack([sym.integral(d["V_chunk"], k1, k2) for k1 in range(nk) for k2 in range(k1 + 1)])
+    pref = -1.0 if ns == 2 else -2.0                   # hf_solver.h:38
+    dm = sym.full_from_ibz(pref * d["G_beta"])
+    S = sym.full_from_ibz(d["S_ibz"])
+    Vh = sym.half_storage(d["V_chunk"])
     with lib.Context(nk, nao, ns, NQ, 2, 2, 2, 100.0) as c:
         c.set_integrals(Vh, lib.INTEGRALS_HF)
         F = c.hf_fock(dm, S, float(d["madelung"]))
-    np.testing.assert_allclose(F[:, sym.ibz2bz], d["Sigma1"], rtol=0, atol=1e-10)
+    np.testing.assert_allclose(sym.ibz_from_full(F), d["Sigma1"], rtol=0, atol=1e-10)
 
 
 def test_dyson_parity(gpu, ctx_small):

@@ -142,7 +142,10 @@ int gb200_create(const gb200_dims* dims, int device, gb200_context** out) {
     return GB200_ERR_INVALID;
   }
   if (d.ns != 1 && d.ns != 2) { g_create_error = "gb200_create: ns must be 1 or 2"; return GB200_ERR_INVALID; }
-  if (d.nso != d.nao) { g_create_error = "gb200_create: two-component (X2C) input is not supported"; return GB200_ERR_INVALID; }
+  if (d.nso != d.nao && !(d.nso == 2 * d.nao && d.ns == 1)) {
+    g_create_error = "gb200_create: nso must equal nao, or 2 nao with ns = 1 (two-component input)";
+    return GB200_ERR_INVALID;
+  }
   if (d.nso > 64) { g_create_error = "gb200_create: nso > 64 is not supported"; return GB200_ERR_INVALID; }
   if (d.nts % 2 != 0) { g_create_error = "Number of tau points should be even!!!"; return GB200_ERR_WRONG_GRID; }
   Context* c = nullptr;

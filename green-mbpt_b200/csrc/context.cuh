@@ -54,7 +54,7 @@ struct Scratch {
 enum ScratchSlot {
   SL_T1 = 0, SL_BT, SL_P0, SL_PW, SL_AUG, SL_TMP, SL_Y1, SL_Y2,
   SL_HF_Y, SL_HF_U, SL_HF_DMT, SL_DY_SW, SL_DY_GW, SL_DY_X, SL_RED, SL_IO_G, SL_IO_S,
-  SL_IO_S1, SL_IO_H, SL_DM, SL_PINV, SL_SPLIT0, SL_COUNT
+  SL_IO_S1, SL_IO_H, SL_DM, SL_PINV, SL_SPLIT0, SL_HF_TAB, SL_X2C_DM, SL_X2C_S, SL_X2C_F, SL_COUNT
 };
 
 struct SplitEngine;

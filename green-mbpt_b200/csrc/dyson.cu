@@ -138,6 +138,7 @@ void tau_to_omega(Context& c, const cplx* Ft, cplx* Fw, cudaStream_t st) {
 
 void dyson_compute_G(Context& c, cplx* Sigma1, cplx* Sigma_tau, double mu, cplx* G, cudaStream_t st) {
   require(c.have_grid && c.have_H, GB200_ERR_STATE, "compute_G: grid and Hamiltonian must be set");
+  require(c.d.nso == c.d.nao, GB200_ERR_INVALID, "compute_G: two-component (X2C) input is supported by the Fock build only");
   const gb200_dims& d = c.d;
   const int64_t nsk = (int64_t)d.ns * d.nk, m2 = (int64_t)d.nso * d.nso;
   hermitize_batched(Sigma1, nsk, d.nso, 1.0, st);                       // dyson.cpp:196
@@ -163,6 +164,7 @@ void dyson_compute_G(Context& c, cplx* Sigma1, cplx* Sigma_tau, double mu, cplx*
 
 void dyson_prepare_X(Context& c, cplx* Sigma1, cplx* Sigma_tau, bool hermitize, cudaStream_t st) {
   require(c.have_grid && c.have_H, GB200_ERR_STATE, "find_mu: grid and Hamiltonian must be set");
+  require(c.d.nso == c.d.nao, GB200_ERR_INVALID, "find_mu: two-component (X2C) input is supported by the Fock build only");
   const gb200_dims& d = c.d;
   const int64_t nsk = (int64_t)d.ns * d.nk, m2 = (int64_t)d.nso * d.nso;
   if (hermitize) {
@@ -247,6 +249,7 @@ double dyson_find_mu(Context& c, double mu0, double nel_target, double tol, doub
 
 void energy(Context& c, const cplx* G, const cplx* Sigma1, const cplx* Sigma_tau, double* e3, cudaStream_t st) {
   require(c.have_grid && c.have_H, GB200_ERR_STATE, "energy: grid and Hamiltonian must be set");
+  require(c.d.nso == c.d.nao, GB200_ERR_INVALID, "energy: two-component (X2C) input is supported by the Fock build only");
   const gb200_dims& d = c.d;
   const int64_t nsk = (int64_t)d.ns * d.nk, m2 = (int64_t)d.nso * d.nso;
   cplx* Gw = (cplx*)c.scratch.get(SL_DY_GW, (size_t)d.nw * nsk * m2 * sizeof(cplx));

@@ -107,6 +107,7 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
   const gb200_dims& d = c.d;
   require(d.nts % 2 == 0, GB200_ERR_WRONG_GRID, "Number of tau points should be even!!!");
   require(c.have_kq && c.have_grid && c.have_V, GB200_ERR_STATE, "gw_sigma: k/q maps, grid and integrals must be set");
+  require(d.nso == d.nao, GB200_ERR_INVALID, "gw_sigma: two-component (X2C) input is supported by the Fock build only");
   const int nk = d.nk, ns = d.ns, nts = d.nts, nth = nts / 2, NQ = d.NQ, nw_b = d.nw_b;
   const int64_t nao = d.nao, nao2 = nao * nao;
   const int64_t pe = c.pair_elems();

@@ -51,7 +51,8 @@ typedef struct gb200_context gb200_context;
 typedef struct {
   int32_t nk;      /* k-points of the full mesh */
   int32_t nao;     /* atomic orbitals */
-  int32_t nso;     /* spin orbitals (== nao; X2C is not supported by the GPU path) */
+  int32_t nso;     /* spin orbitals: nao, or 2 nao with ns = 1 for two-component (X2C) input,
+                      which the Fock build accepts (the GW and Dyson entry points reject it) */
   int32_t ns;      /* spin channels, 1 or 2 */
   int32_t NQ;      /* auxiliary basis size */
   int32_t nts;     /* tau points (even) */
@@ -112,8 +113,9 @@ int gb200_gw_sigma_device(gb200_context* ctx, const double* G_dev, double* Sigma
 
 /* Hartree-Fock Fock matrix F [ns, nk, nso, nso] from the density matrix dm
  * and overlap S (same shape).  Replaces hf_scalar_cpu_kernel::solve
- * (hf_cpu_kernels.cpp:25-146); dm = spin_prefactor * G(beta) as in
- * hf_solver::solve (hf_solver.cpp:9-16). */
+ * (hf_cpu_kernels.cpp:25-146) and, for nso = 2 nao, hf_x2c_cpu_kernel::solve
+ * (:148-279); dm = spin_prefactor * G(beta) as in hf_solver::solve
+ * (hf_solver.cpp:9-16). */
 int gb200_hf_fock(gb200_context* ctx, const double* dm, const double* S, double madelung, double* F);
 int gb200_hf_fock_device(gb200_context* ctx, const double* dm_dev, const double* S_dev, double madelung,
                          double* F_dev, void* stream);

@@ -155,3 +155,46 @@ def test_device_integrals_in_chunks_match_host_upload(gpu):
         torch.cuda.synchronize()
         got = c.gw_sigma(s.G)
     assert rel(got, want) < 1e-14
+
+
+def test_hf_x2c_golden_through_gpu(gpu):
+    """Two-component (X2C) Fock build on the GPU against the reference's HF_X2C fixture
+    (hf_x2c_cpu_kernel::solve, hf_cpu_kernels.cpp:148-279), at the reference's 1e-10."""
+    from gb200 import inputs
+    d = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "hf_x2c.npz")))
+    sym = inputs.KSymmetry(d["bz2ibz"], d["ibz2bz"], d["tr_conj"], d["k_sym_transform_ao"], d["conj_pairs_list"],
+                           d["trans_pairs_list"], d["kpair_irre_list"], d["weight_ibz"])
+    ns, nk, nao, nso, NQ = int(d["ns"]), int(d["nk"]), int(d["nao"]), int(d["nso"]), int(d["NQ"])
+    assert nso == 2 * nao and ns == 1
+    dm = sym.full_from_ibz(-1.0 * d["G_beta"])         # spin_prefactor -1 for X2C (hf_solver.h:38)
+    S = sym.full_from_ibz(d["S_ibz"])
+    with lib.Context(nk, nao, ns, NQ, 2, 2, 2, 100.0, nso=nso) as c:
+        c.set_integrals(sym.half_storage(d["V_chunk"]), lib.INTEGRALS_HF)
+        F = c.hf_fock(dm, S, float(d["madelung"]))
+        with pytest.raises(lib.mbpt_kernel_error):
+            c.gw_sigma(np.zeros((2, ns, nk, nso, nso), dtype=np.complex128))
+    np.testing.assert_allclose(sym.ibz_from_full(F), d["Sigma1"], rtol=0, atol=1e-10)
+    # Hermitian to round-off (the reference does not hermitize the diagonal blocks either)
+    assert np.abs(F - np.conj(np.swapaxes(F, -1, -2))).max() < 1e-11 * np.abs(F).max()
+
+
+def test_hf_x2c_matches_oracle_with_madelung(gpu):
+    """X2C Fock build with a non-zero Madelung constant and several k-points against the oracle."""
+    s = system("small")
+    nk, nao, NQ = s.nk, s.nao, s.NQ
+    rng = np.random.default_rng(3)
+    nso = 2 * nao
+    a = rng.standard_normal((1, nk, nso, nso)) + 1j * rng.standard_normal((1, nk, nso, nso))
+    dm = 0.05 * (a + np.conj(np.swapaxes(a, -1, -2)))
+    b = rng.standard_normal((nk, nao, nao)) + 1j * rng.standard_normal((nk, nao, nao))
+    Saa = np.eye(nao) + 0.02 * (b + np.conj(np.swapaxes(b, -1, -2)))
+    S = np.zeros((1, nk, nso, nso), dtype=np.complex128)
+    S[0, :, :nao, :nao] = Saa
+    S[0, :, nao:, nao:] = Saa
+    mad = 0.21
+    integ = O.HalfStoredIntegrals(s.V_half)
+    want = O.hf_x2c(dm, S, mad, integ.pair, lambda X, k: X[k], nk, lambda ik: ik, NQ, nao)
+    with lib.Context(nk, nao, 1, NQ, 2, 2, 2, 20.0, nso=nso) as c:
+        c.set_integrals(s.V_half, lib.INTEGRALS_HF)
+        F = c.hf_fock(dm, S, mad)
+    assert rel(F, want) < TOL

@@ -54,7 +54,8 @@ struct Scratch {
 enum ScratchSlot {
   SL_T1 = 0, SL_BT, SL_P0, SL_PW, SL_AUG, SL_TMP, SL_Y1, SL_Y2,
   SL_HF_Y, SL_HF_U, SL_HF_DMT, SL_DY_SW, SL_DY_GW, SL_DY_X, SL_RED, SL_IO_G, SL_IO_S,
-  SL_IO_S1, SL_IO_H, SL_DM, SL_PINV, SL_SPLIT0, SL_HF_TAB, SL_X2C_DM, SL_X2C_S, SL_X2C_F, SL_COUNT
+  SL_IO_S1, SL_IO_H, SL_DM, SL_PINV, SL_SPLIT0, SL_HF_TAB, SL_X2C_DM, SL_X2C_S, SL_X2C_F, SL_X2C_GAB, SL_X2C_GBA,
+  SL_X2C_SIG, SL_COUNT
 };
 
 struct SplitEngine;
@@ -107,6 +108,9 @@ struct Context {
 
   int64_t nao() const { return d.nao; }
   int64_t pair_elems() const { return (int64_t)d.NQ * d.nao * d.nao; }
+  // two-component (X2C) input: nso = 2 nao, the GW contractions run over the 4 spin blocks
+  bool x2c() const { return d.nso == 2 * d.nao; }
+  int ns_eff() const { return x2c() ? 4 : d.ns; }
   int64_t g_elems() const { return (int64_t)d.nts * d.ns * d.nk * d.nso * d.nso; }
   int64_t mat_elems() const { return (int64_t)d.ns * d.nk * d.nso * d.nso; }
 };

@@ -43,6 +43,34 @@ __global__ void symmetrize_p0_kernel(cplx* P0, int nts, int NQ, double inv_nk) {
   }
 }
 
+// Two-component G [nts][nk][2n][2n] -> spin blocks Gab[t][s][k] = G(t,k)[a-block, b-block] and
+// Gba[t][s][k] = G(t,k)[b-block, a-block] for s = 2a + b (gw_cpu_kernel.cpp:166-187: G(k+q) takes
+// block (a,b), Gbar(k) block (b,a))
+__global__ void x2c_pack_g_kernel(const cplx* G, cplx* Gab, cplx* Gba, int nts, int nk, int n) {
+  const int64_t n2 = (int64_t)n * n, so = 2 * (int64_t)n;
+  const int64_t total = (int64_t)nts * 4 * nk * n2;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e % n2, i = r / n, j = r % n;
+    const int64_t k = (e / n2) % nk, s = (e / (n2 * nk)) % 4, t = e / (n2 * nk * 4);
+    const int64_t a = s / 2, b = s % 2;
+    const cplx* M = G + (t * nk + k) * so * so;
+    Gab[e] = M[(a * n + i) * so + b * n + j];
+    Gba[e] = M[(b * n + i) * so + a * n + j];
+  }
+}
+
+// spin-block self-energy Sps[t][s][k] -> two-component Sigma [nts][nk][2n][2n], block (a,b)
+__global__ void x2c_unpack_sigma_kernel(const cplx* Sps, cplx* Sigma, int nts, int nk, int n) {
+  const int64_t n2 = (int64_t)n * n, so = 2 * (int64_t)n;
+  const int64_t total = (int64_t)nts * 4 * nk * n2;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e % n2, i = r / n, j = r % n;
+    const int64_t k = (e / n2) % nk, s = (e / (n2 * nk)) % 4, t = e / (n2 * nk * 4);
+    const int64_t a = s / 2, b = s % 2;
+    Sigma[(t * nk + k) * so * so + (a * n + i) * so + b * n + j] = Sps[e];
+  }
+}
+
 inline unsigned grid_for(int64_t n, int nt) {
   int64_t g = (n + nt - 1) / nt;
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
@@ -60,9 +88,11 @@ ZOperand dense(const cplx* p, int64_t ld) {
 }  // namespace
 
 void build_tables(Context& c) {
-  const int nk = c.d.nk, ns = c.d.ns;
+  // G offsets address the spin-block layout the contractions read: [t][s][k][nao][nao] (for
+  // two-component input the 4 spin blocks repacked by gw_sigma)
+  const int nk = c.d.nk, ns = c.ns_eff();
   const int64_t pe = c.pair_elems();
-  const int64_t ge = (int64_t)c.d.nso * c.d.nso;
+  const int64_t ge = (int64_t)c.d.nao * c.d.nao;
   std::vector<int64_t> pp(nk * nk), pm(nk * nk), gp(nk * nk), gm(nk * nk), ppns((size_t)nk * nk * ns);
   for (int q = 0; q < nk; ++q)
     for (int k = 0; k < nk; ++k) {
@@ -107,21 +137,35 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
   const gb200_dims& d = c.d;
   require(d.nts % 2 == 0, GB200_ERR_WRONG_GRID, "Number of tau points should be even!!!");
   require(c.have_kq && c.have_grid && c.have_V, GB200_ERR_STATE, "gw_sigma: k/q maps, grid and integrals must be set");
-  require(d.nso == d.nao, GB200_ERR_INVALID, "gw_sigma: two-component (X2C) input is supported by the Fock build only");
-  const int nk = d.nk, ns = d.ns, nts = d.nts, nth = nts / 2, NQ = d.NQ, nw_b = d.nw_b;
+  // two-component input: the contractions run over the 4 spin blocks of G (pseudo spins,
+  // gw_cpu_kernel.cpp:166-168,326-327) on a repacked copy, prefactor 1
+  const bool x2c = c.x2c();
+  const int nk = d.nk, ns = c.ns_eff(), nts = d.nts, nth = nts / 2, NQ = d.NQ, nw_b = d.nw_b;
   const int64_t nao = d.nao, nao2 = nao * nao;
   const int64_t pe = c.pair_elems();
   const int64_t ge = nao2;                         // one G matrix
   const int64_t g_s = (int64_t)nk * ge;            // stride of spin in G
   const int64_t g_t = (int64_t)ns * g_s;           // stride of tau in G
-  const double pref = (ns == 2) ? 1.0 : 2.0;       // gw_cpu_kernel.cpp:167 (no X2C)
+  const double pref = (d.ns == 2 || x2c) ? 1.0 : 2.0;  // gw_cpu_kernel.cpp:167
+  cplx* Sigma_out = Sigma;
+  const cplx* Gbar = G;  // the operand of Gbar(beta - tau, k): block (b,a) for two-component input
+  if (x2c) {
+    const int64_t n = (int64_t)nts * 4 * nk * nao2;
+    cplx* Gab = (cplx*)c.scratch.get(SL_X2C_GAB, (size_t)n * sizeof(cplx));
+    cplx* Gba = (cplx*)c.scratch.get(SL_X2C_GBA, (size_t)n * sizeof(cplx));
+    x2c_pack_g_kernel<<<grid_for(n, 256), 256, 0, st>>>(G, Gab, Gba, nts, nk, (int)nao);
+    GB_CHECK_LAUNCH();
+    G = Gab;
+    Gbar = Gba;
+    Sigma = (cplx*)c.scratch.get(SL_X2C_SIG, (size_t)n * sizeof(cplx));
+  }
   const bool split = c.prec_mode == GB200_PREC_SPLIT;
 
   for (int i = 0; i < 5; ++i)
     if (!c.ev[i]) GB_CUDA(cudaEventCreate(&c.ev[i]));
   GB_CUDA(cudaEventRecord(c.ev[0], st));
 
-  GB_CUDA(cudaMemsetAsync(Sigma, 0, c.g_elems() * sizeof(cplx), st));
+  GB_CUDA(cudaMemsetAsync(Sigma, 0, (size_t)nts * ns * nk * nao2 * sizeof(cplx), st));
   const int64_t per_k_sigma = (int64_t)nts * ns * pe;
   const int kb = choose_kblock(c, per_k_sigma);
   cplx* P0 = (cplx*)c.scratch.get(SL_P0, (size_t)nts * NQ * NQ * sizeof(cplx));
@@ -167,7 +211,7 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
       ZGemm b;
       b.M = nao; b.N = (int64_t)NQ * nao; b.K = nao;
       b.nb0 = kbk; b.nb1 = nth; b.nb2 = ns;
-      b.A = dense(G + (int64_t)(nts - 1) * g_t + (int64_t)k0 * ge, nao);
+      b.A = dense(Gbar + (int64_t)(nts - 1) * g_t + (int64_t)k0 * ge, nao);
       b.A.bat.s0 = ge; b.A.bat.s1 = -g_t; b.A.bat.s2 = g_s;
       b.B.ptr = X1; b.B.row = lin(nao); b.B.col = two(nao, 1, nao2);
       b.B.bat.s0 = blkT1; b.B.bat.s1 = (int64_t)ns * pe; b.B.bat.s2 = pe;
@@ -270,7 +314,12 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
     GB_CUDA(cudaEventElapsedTime(&c_ms, c.ev[3], c.ev[4]));
     t_p0 += a_ms; t_w += b_ms; t_sig += c_ms;
   }
-  scale_inplace(Sigma, c.g_elems(), 1.0 / nk, st);  // gw_cpu_kernel.cpp:55
+  scale_inplace(Sigma, (int64_t)nts * ns * nk * nao2, 1.0 / nk, st);  // gw_cpu_kernel.cpp:55
+  if (x2c) {
+    const int64_t n = (int64_t)nts * 4 * nk * nao2;
+    x2c_unpack_sigma_kernel<<<grid_for(n, 256), 256, 0, st>>>(Sigma, Sigma_out, nts, nk, (int)nao);
+    GB_CHECK_LAUNCH();
+  }
   if (se) {
     int e = split_check_error(c, st);
     require(e == 0, GB200_ERR_CUDA, "split contraction: tensor-core pipeline wait timed out (code " + std::to_string(e) + ")");

@@ -198,3 +198,29 @@ def test_hf_x2c_matches_oracle_with_madelung(gpu):
         c.set_integrals(s.V_half, lib.INTEGRALS_HF)
         F = c.hf_fock(dm, S, mad)
     assert rel(F, want) < TOL
+
+
+@pytest.mark.parametrize("prec", [lib.PREC_FP64, lib.PREC_SPLIT])
+def test_gw_x2c_matches_oracle(gpu, prec):
+    """Two-component (X2C) GW self-energy: the 4 spin blocks of G (gw_cpu_kernel.cpp:166-187,
+    326-351) against the oracle; FP64 at 1e-10, split precision (S = 5) at 1e-8."""
+    s = system("small")
+    nk, nao, NQ, g = s.nk, s.nao, s.NQ, s.grid
+    rng = np.random.default_rng(7)
+    nso = 2 * nao
+    G2 = np.zeros((g.nts, 1, nk, nso, nso), dtype=np.complex128)
+    X = rng.standard_normal((nk, nao, nao)) + 1j * rng.standard_normal((nk, nao, nao))
+    for t in range(g.nts):
+        G2[t, 0, :, :nao, :nao] = s.G[t, 0]
+        G2[t, 0, :, nao:, nao:] = 0.7 * s.G[t, 0]
+        G2[t, 0, :, :nao, nao:] = 0.05 * X
+        G2[t, 0, :, nao:, :nao] = 0.05 * np.conj(np.swapaxes(X, -1, -2))
+    want = O.gw_solve(G2, O.HalfStoredIntegrals(s.V_half), O.NoSymBZ(s.mesh), g.Tnt_b, g.Ttn_b, 1, NQ, X2C=True)
+    with lib.Context(nk, nao, 1, NQ, g.nts, g.nw, g.nw_b, s.beta, nso=nso) as c:
+        kp, km = solvers.kq_maps(s.mesh)
+        c.set_kq_maps(kp, km)
+        c.set_grid(g.Tnt_f, g.Ttn_f, g.Tnt_b, g.Ttn_b, g.wsample_f)
+        c.set_integrals(s.V_half, lib.INTEGRALS_GW)
+        c.set_precision(prec, 5)
+        got = c.gw_sigma(G2)
+    assert rel(got, want) < (TOL if prec == lib.PREC_FP64 else 1e-8)

@@ -383,7 +383,7 @@ int gb200_iteration_device(gb200_context* ctx, double* G_dev, double* Sigma1_dev
     // dm = spin_prefactor * G(beta) (hf_solver.cpp:9-16)
     cplx* dm = (cplx*)c.scratch.get(SL_DM, me * sizeof(cplx));
     GB_CUDA(cudaMemcpyAsync(dm, G + (int64_t)(d.nts - 1) * me, me * sizeof(cplx), cudaMemcpyDeviceToDevice, st));
-    scale_inplace(dm, me, d.ns == 2 ? -1.0 : -2.0, st);
+    scale_inplace(dm, me, (d.ns == 2 || c.x2c()) ? -1.0 : -2.0, st);
     require(c.have_H, GB200_ERR_STATE, "iteration: Hamiltonian/overlap must be set");
     hf_fock(c, dm, c.S.get(), madelung, S1, st);
     gw_sigma(c, G, St, st);

@@ -138,7 +138,6 @@ void tau_to_omega(Context& c, const cplx* Ft, cplx* Fw, cudaStream_t st) {
 
 void dyson_compute_G(Context& c, cplx* Sigma1, cplx* Sigma_tau, double mu, cplx* G, cudaStream_t st) {
   require(c.have_grid && c.have_H, GB200_ERR_STATE, "compute_G: grid and Hamiltonian must be set");
-  require(c.d.nso == c.d.nao, GB200_ERR_INVALID, "compute_G: two-component (X2C) input is supported by the Fock build only");
   const gb200_dims& d = c.d;
   const int64_t nsk = (int64_t)d.ns * d.nk, m2 = (int64_t)d.nso * d.nso;
   hermitize_batched(Sigma1, nsk, d.nso, 1.0, st);                       // dyson.cpp:196
@@ -164,7 +163,6 @@ void dyson_compute_G(Context& c, cplx* Sigma1, cplx* Sigma_tau, double mu, cplx*
 
 void dyson_prepare_X(Context& c, cplx* Sigma1, cplx* Sigma_tau, bool hermitize, cudaStream_t st) {
   require(c.have_grid && c.have_H, GB200_ERR_STATE, "find_mu: grid and Hamiltonian must be set");
-  require(c.d.nso == c.d.nao, GB200_ERR_INVALID, "find_mu: two-component (X2C) input is supported by the Fock build only");
   const gb200_dims& d = c.d;
   const int64_t nsk = (int64_t)d.ns * d.nk, m2 = (int64_t)d.nso * d.nso;
   if (hermitize) {
@@ -199,7 +197,7 @@ double dyson_electrons_prepared(Context& c, double mu, cudaStream_t st) {
   GB_CUDA(cudaStreamSynchronize(st));
   double re = 0.0;
   for (int n = 0; n < d.nw; ++n) re += cmul(c.Ttn_beta[n], tw[n]).x;
-  const double prefactor = (d.ns == 2) ? 1.0 : 2.0;  // dyson.cpp:95
+  const double prefactor = (d.ns == 2 || c.x2c()) ? 1.0 : 2.0;  // dyson.cpp:95
   return prefactor * -re;
 }
 
@@ -249,7 +247,6 @@ double dyson_find_mu(Context& c, double mu0, double nel_target, double tol, doub
 
 void energy(Context& c, const cplx* G, const cplx* Sigma1, const cplx* Sigma_tau, double* e3, cudaStream_t st) {
   require(c.have_grid && c.have_H, GB200_ERR_STATE, "energy: grid and Hamiltonian must be set");
-  require(c.d.nso == c.d.nao, GB200_ERR_INVALID, "energy: two-component (X2C) input is supported by the Fock build only");
   const gb200_dims& d = c.d;
   const int64_t nsk = (int64_t)d.ns * d.nk, m2 = (int64_t)d.nso * d.nso;
   cplx* Gw = (cplx*)c.scratch.get(SL_DY_GW, (size_t)d.nw * nsk * m2 * sizeof(cplx));
@@ -260,7 +257,7 @@ void energy(Context& c, const cplx* G, const cplx* Sigma1, const cplx* Sigma_tau
   trace_product_kernel<<<d.nw, 256, 0, st>>>(Gw, Sw, true, red, nsk, d.nso, 1.0);
   GB_CHECK_LAUNCH();
   double* h2 = (double*)(red + d.nw);
-  const double dm_pref = (d.ns == 2) ? -1.0 : -2.0;
+  const double dm_pref = (d.ns == 2 || c.x2c()) ? -1.0 : -2.0;  // common_utils.cpp:18
   hf_energy_kernel<<<1, 256, 0, st>>>(G + (int64_t)(d.nts - 1) * nsk * m2, Sigma1, c.H.get(), dm_pref, nsk, d.nso, h2);
   GB_CHECK_LAUNCH();
   std::vector<cplx> gs(d.nw);
@@ -270,7 +267,7 @@ void energy(Context& c, const cplx* G, const cplx* Sigma1, const cplx* Sigma_tau
   GB_CUDA(cudaStreamSynchronize(st));
   double re = 0.0;
   for (int n = 0; n < d.nw; ++n) re += cmul(c.Ttn_beta[n], gs[n]).x;
-  const double e_pref = (d.ns == 1) ? 1.0 : 0.5;  // common_utils.cpp:31
+  const double e_pref = (d.ns == 1 && !c.x2c()) ? 1.0 : 0.5;  // common_utils.cpp:37
   const double nkpw = 1.0 / d.nk;
   e3[0] = hh[1] * nkpw;               // E_1b
   e3[1] = 0.5 * hh[0] * nkpw;         // E_HF

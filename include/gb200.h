@@ -51,9 +51,8 @@ typedef struct gb200_context gb200_context;
 typedef struct {
   int32_t nk;      /* k-points of the full mesh */
   int32_t nao;     /* atomic orbitals */
-  int32_t nso;     /* spin orbitals: nao, or 2 nao with ns = 1 for two-component (X2C) input,
-                      which the Fock build and the GW self-energy accept (the Dyson and
-                      energy entry points reject it) */
+  int32_t nso;     /* spin orbitals: nao, or 2 nao with ns = 1 for two-component (X2C) input
+                      (spinor blocks aa, ab, ba, bb of nao x nao; integrals stay nao x nao) */
   int32_t ns;      /* spin channels, 1 or 2 */
   int32_t NQ;      /* auxiliary basis size */
   int32_t nts;     /* tau points (even) */

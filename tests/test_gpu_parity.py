@@ -224,3 +224,43 @@ def test_gw_x2c_matches_oracle(gpu, prec):
         c.set_precision(prec, 5)
         got = c.gw_sigma(G2)
     assert rel(got, want) < (TOL if prec == lib.PREC_FP64 else 1e-8)
+
+
+def test_dyson_x2c_matches_oracle(gpu):
+    """Dyson step, electron count, chemical potential and energies for two-component input
+    (prefactors of dyson.cpp:95 and common_utils.cpp:18,37 with X2C) against the oracle."""
+    s = system("small")
+    nk, nao, g = s.nk, s.nao, s.grid
+    nso = 2 * nao
+    rng = np.random.default_rng(11)
+
+    def herm(shape, scale):
+        a = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+        return scale * (a + np.conj(np.swapaxes(a, -1, -2)))
+
+    H = np.zeros((1, nk, nso, nso), dtype=np.complex128)
+    S = np.zeros_like(H)
+    H[0, :, :nao, :nao] = s.F[0]
+    H[0, :, nao:, nao:] = s.F[0]
+    H[0] += herm((nk, nso, nso), 0.02)
+    S[0, :, :nao, :nao] = s.S[0]
+    S[0, :, nao:, nao:] = s.S[0]
+    F1 = herm((1, nk, nso, nso), 0.05)
+    sig = herm((g.nts, 1, nk, nso, nso), 0.01)
+    with lib.Context(nk, nao, 1, s.NQ, g.nts, g.nw, g.nw_b, s.beta, nso=nso) as c:
+        c.set_grid(g.Tnt_f, g.Ttn_f, g.Tnt_b, g.Ttn_b, g.wsample_f)
+        c.set_hamiltonian(H, S)
+        mu = -0.2
+        G, _, _ = c.compute_G(F1, sig, mu)
+        Gref = O.compute_G(F1, sig, H, S, mu, g.Tnt_f, g.Ttn_f, g.wsample_f)
+        assert rel(G, Gref) < TOL
+        ev = O.selfenergy_eigenspectra(F1, sig, H, S, g.Tnt_f)
+        n_ref = O.number_of_electrons(mu, ev, g.Ttn_beta, g.wsample_f, 1, 1.0 / nk, X2C=True)
+        assert abs(c.electrons(F1, sig, mu) - n_ref) < 1e-10 * abs(n_ref)
+        target = n_ref + 0.5
+        nel_g, mu_g = c.find_mu(F1, sig, 0.0, target, 1e-9)
+        nel_o, mu_o = O.find_mu(0.0, target, ev, g.Ttn_beta, g.wsample_f, 1, 1.0 / nk, 1e-9, X2C=True)
+        assert abs(mu_g - mu_o) < 1e-8
+        e_gpu = c.energy(Gref, F1, sig)
+    e_ref = O.compute_energy(Gref, F1, sig, H, g.Tnt_f, g.Ttn_beta, 1.0 / nk, X2C=True)
+    np.testing.assert_allclose(e_gpu, e_ref, rtol=1e-10, atol=1e-12)

@@ -62,14 +62,12 @@ def context_from_files(input_path: str, hf_integrals: str | None = None, gw_inte
     inp = inputs.read_input(input_path)
     sym = inp["symmetry"]
     nk, nao, nso, ns, NQ = inp["nk"], inp["nao"], inp["nso"], inp["ns"], inp["NQ"]
-    if nso != nao:
-        raise lib.mbpt_kernel_error("two-component (X2C) inputs are not supported by the GPU kernels")
     if grid is not None:
         ctx = lib.Context(nk, nao, ns, NQ, grid.nts, grid.nw, grid.nw_b, float(beta if beta is not None else grid.beta),
-                          device=device)
+                          nso=nso, device=device)
         ctx.set_grid(grid.Tnt_f, grid.Ttn_f, grid.Tnt_b, grid.Ttn_b, grid.wsample_f)
     else:
-        ctx = lib.Context(nk, nao, ns, NQ, 2, 2, 3, float(beta or 1.0), device=device)
+        ctx = lib.Context(nk, nao, ns, NQ, 2, 2, 3, float(beta or 1.0), nso=nso, device=device)
     if inp.get("k_frac") is not None:
         kp, km = inputs.kq_maps_from_points(inp["k_frac"])
         ctx.set_kq_maps(kp, km)

@@ -214,6 +214,8 @@ int gb200_set_grid(gb200_context* ctx, const double* Tnt_f, const double* Ttn_f,
     c.wsample_f.assign(wsample_f, wsample_f + d.nw);
     const cplx* tb = reinterpret_cast<const cplx*>(Ttn_f) + (size_t)(d.nts - 1) * d.nw;
     c.Ttn_beta.assign(tb, tb + d.nw);
+    const cplx* tbb = reinterpret_cast<const cplx*>(Ttn_b);
+    c.Ttn_b_host.assign(tbb, tbb + (size_t)d.nts * d.nw_b);
     GB_CUDA(cudaStreamSynchronize(c.stream));
     c.have_grid = true;
   });
@@ -433,6 +435,22 @@ int gb200_set_integrals_device(gb200_context* ctx, int which, const double* V_de
     } else {
       c.have_Vhf = done >= npairs;
     }
+  });
+}
+
+int gb200_set_q0_correction(gb200_context* ctx, const double* AqQ, const double* q_abs, double madelung) {
+  return guarded(ctx, [&](Context& c) {
+    if (!AqQ) {
+      c.q0_on = false;
+      return;
+    }
+    require(q_abs != nullptr, GB200_ERR_INVALID, "set_q0_correction: null pointer");
+    const int nq = c.d.nk;
+    c.AqQ.upload(reinterpret_cast<const cplx*>(AqQ), (size_t)nq * c.d.NQ, c.stream);
+    c.q_abs.assign(q_abs, q_abs + nq);
+    c.q0_madelung = madelung;
+    GB_CUDA(cudaStreamSynchronize(c.stream));
+    c.q0_on = true;
   });
 }
 

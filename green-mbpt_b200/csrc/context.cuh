@@ -55,7 +55,7 @@ enum ScratchSlot {
   SL_T1 = 0, SL_BT, SL_P0, SL_PW, SL_AUG, SL_TMP, SL_Y1, SL_Y2,
   SL_HF_Y, SL_HF_U, SL_HF_DMT, SL_DY_SW, SL_DY_GW, SL_DY_X, SL_RED, SL_IO_G, SL_IO_S,
   SL_IO_S1, SL_IO_H, SL_DM, SL_PINV, SL_SPLIT0, SL_HF_TAB, SL_X2C_DM, SL_X2C_S, SL_X2C_F, SL_X2C_GAB, SL_X2C_GBA,
-  SL_X2C_SIG, SL_COUNT
+  SL_X2C_SIG, SL_Q0_Y, SL_Q0_T, SL_Q0_D, SL_Q0_E, SL_Q0_S, SL_COUNT
 };
 
 struct SplitEngine;
@@ -84,6 +84,13 @@ struct Context {
   DevArray<cplx> Tnt_f, Ttn_f, Tnt_b, Ttn_b;
   std::vector<double> wsample_f;
   std::vector<cplx> Ttn_beta;  // host copy of the tau = beta row of Ttn_f
+  std::vector<cplx> Ttn_b_host;  // host copy of Ttn_b [nts][nw_b]
+  // q -> 0 correction ("extrapolate" treatment, mbpt_q0_utils_t): AqQ [nk][NQ] on the device,
+  // |q| on the host, the Madelung constant; eps_inv [nw_b][nk] collects the heads of P(i Omega, q)
+  bool q0_on = false;
+  DevArray<cplx> AqQ, eps_inv;
+  std::vector<double> q_abs;
+  double q0_madelung = 0.0;
 
   // integrals, all ordered pairs [nk][nk][NQ][nao][nao]
   DevArray<cplx> V, Vhf;
@@ -119,6 +126,8 @@ struct Context {
 void build_tables(Context& c);
 void build_hf_tables(Context& c);
 void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st);
+// q -> 0 limit of the collected heads eps_inv[nw_b][nq] (mbpt_q0_utils_t.cpp:30-86), on the host
+cplx extrapolate_q0(const cplx* eps_n, const std::vector<double>& q_abs, int fit_order, double q_max);
 void hf_fock(Context& c, const cplx* dm, const cplx* S, double madelung, cplx* F, cudaStream_t st);
 void dyson_compute_G(Context& c, cplx* Sigma1, cplx* Sigma_tau, double mu, cplx* G, cudaStream_t st);
 void dyson_prepare_X(Context& c, cplx* Sigma1, cplx* Sigma_tau, bool hermitize, cudaStream_t st);

@@ -12,6 +12,8 @@
 //    which is the same sum, P0_QQ' = -pref sum Gbar_tp V^Q_pm G_mn conj(V^Q'_tn),
 //    Sigma_ij = -sum V^Q_im G_mn W_QQ' conj(V^Q'_jn), in a batched order.
 #include <algorithm>
+#include <cmath>
+#include <vector>
 
 #include "context.cuh"
 #include "split.cuh"
@@ -69,6 +71,39 @@ __global__ void x2c_unpack_sigma_kernel(const cplx* Sps, cplx* Sigma, int nts, i
     const int64_t a = s / 2, b = s % 2;
     Sigma[(t * nk + k) * so * so + (a * n + i) * so + b * n + j] = Sps[e];
   }
+}
+
+// S2[k] = block-diag(S_aa(k), S_aa(k)) from two-component S [nk][2n][2n] (the q -> 0 correction
+// of two-component input uses the AO overlap S_aa on every spin block, mbpt_q0_utils_t.cpp:142-171)
+__global__ void q0_x2c_overlap_kernel(const cplx* S, cplx* S2, int nk, int n) {
+  const int64_t so = 2 * (int64_t)n, total = (int64_t)nk * so * so;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = e / (so * so), r = e % (so * so), i = r / so, j = r % so;
+    const bool diag = (i < n) == (j < n);
+    S2[e] = diag ? S[k * so * so + (i % n) * so + (j % n)] : cmk(0.0, 0.0);
+  }
+}
+
+// T[t] *= coef[t] for T [nts][per_t]
+__global__ void q0_scale_kernel(cplx* T, const cplx* coef, int nts, int64_t per_t) {
+  const int64_t total = (int64_t)nts * per_t;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x)
+    T[e] = cmul(coef[e / per_t], T[e]);
+}
+
+// two-component correction: block ba = (block ab)^H (mbpt_q0_utils_t.cpp:164-168)
+__global__ void q0_x2c_offdiag_kernel(cplx* D, int64_t nmat, int n) {
+  const int64_t so = 2 * (int64_t)n, n2 = (int64_t)n * n, total = nmat * n2;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t m = e / n2, r = e % n2, i = r / n, j = r % n;
+    cplx* M = D + m * so * so;
+    M[(j + n) * so + i] = cconj(M[i * so + (j + n)]);
+  }
+}
+
+__global__ void add_kernel(cplx* Y, const cplx* X, int64_t count) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < count; e += (int64_t)gridDim.x * blockDim.x)
+    Y[e] = cadd(Y[e], X[e]);
 }
 
 inline unsigned grid_for(int64_t n, int nt) {
@@ -133,6 +168,113 @@ static int choose_kblock(const Context& c, int64_t elems_per_k) {
   return std::min(kb, c.d.nk);
 }
 
+cplx extrapolate_q0(const cplx* eps_n, const std::vector<double>& q_abs, int fit_order, double q_max) {
+  // first occurrence of every distinct |q| in (0, q_max] (filter_q_abs), quadratic least squares
+  // by the normal equations solved with full pivoting (polyfit); rank-deficient systems take 0
+  // for the undetermined coefficients
+  std::vector<double> x, y;
+  for (size_t i = 0; i < q_abs.size(); ++i) {
+    const double qa = q_abs[i];
+    if (!(qa > 0.0 && qa <= q_max)) continue;
+    if (std::find(x.begin(), x.end(), qa) != x.end()) continue;
+    x.push_back(qa);
+    y.push_back(eps_n[i].x);
+  }
+  const int m = fit_order + 1;
+  std::vector<double> A((size_t)m * m, 0.0), b(m, 0.0);
+  for (size_t i = 0; i < x.size(); ++i) {
+    std::vector<double> row(m);
+    for (int j = 0; j < m; ++j) row[j] = std::pow(x[i], j);
+    for (int r = 0; r < m; ++r) {
+      b[r] += row[r] * y[i];
+      for (int cc = 0; cc < m; ++cc) A[r * m + cc] += row[r] * row[cc];
+    }
+  }
+  std::vector<int> colp(m);
+  for (int j = 0; j < m; ++j) colp[j] = j;
+  double amax = 0.0;
+  for (double v : A) amax = std::max(amax, std::fabs(v));
+  int rank = 0;
+  for (int piv = 0; piv < m; ++piv) {
+    int pr = piv, pc = piv;
+    double best = -1.0;
+    for (int r = piv; r < m; ++r)
+      for (int cc = piv; cc < m; ++cc)
+        if (std::fabs(A[r * m + cc]) > best) { best = std::fabs(A[r * m + cc]); pr = r; pc = cc; }
+    if (best <= 1e-14 * amax || best == 0.0) break;
+    for (int cc = 0; cc < m; ++cc) std::swap(A[piv * m + cc], A[pr * m + cc]);
+    std::swap(b[piv], b[pr]);
+    for (int r = 0; r < m; ++r) std::swap(A[r * m + piv], A[r * m + pc]);
+    std::swap(colp[piv], colp[pc]);
+    for (int r = piv + 1; r < m; ++r) {
+      const double f = A[r * m + piv] / A[piv * m + piv];
+      for (int cc = piv; cc < m; ++cc) A[r * m + cc] -= f * A[piv * m + cc];
+      b[r] -= f * b[piv];
+    }
+    ++rank;
+  }
+  std::vector<double> z(m, 0.0);
+  for (int r = rank - 1; r >= 0; --r) {
+    double v = b[r];
+    for (int cc = r + 1; cc < rank; ++cc) v -= A[r * m + cc] * z[cc];
+    z[r] = v / A[r * m + r];
+  }
+  std::vector<double> coef(m, 0.0);
+  for (int j = 0; j < m; ++j) coef[colp[j]] = z[j];
+  return cmk(coef[0], 0.0);
+}
+
+// Sigma += -madelung eps_inv_q0(t) S G(t) S (GW_q0_correction, mbpt_q0_utils_t.cpp:88-178)
+static void apply_q0(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
+  const gb200_dims& d = c.d;
+  require(c.have_H, GB200_ERR_STATE, "q0 correction: the overlap (gb200_dyson_set_hamiltonian) must be set");
+  const int nk = d.nk, nts = d.nts, nw_b = d.nw_b;
+  const int64_t nso = d.nso, m2 = nso * nso, nmat = (int64_t)d.ns * nk;
+  std::vector<cplx> eps((size_t)nw_b * nk);
+  GB_CUDA(cudaMemcpyAsync(eps.data(), c.eps_inv.get(), eps.size() * sizeof(cplx), cudaMemcpyDeviceToHost, st));
+  GB_CUDA(cudaStreamSynchronize(st));
+  std::vector<cplx> ew(nw_b), coef(nts);
+  for (int n = 0; n < nw_b; ++n) ew[n] = extrapolate_q0(eps.data() + (size_t)n * nk, c.q_abs, 2, 1.0);
+  for (int t = 0; t < nts; ++t) {
+    cplx acc = cmk(0.0, 0.0);
+    for (int n = 0; n < nw_b; ++n) acc = cadd(acc, cmul(c.Ttn_b_host[(size_t)t * nw_b + n], ew[n]));
+    coef[t] = cscale(acc, -c.q0_madelung);
+  }
+  cplx* dcoef = (cplx*)c.scratch.get(SL_Q0_E, (size_t)nts * sizeof(cplx));
+  GB_CUDA(cudaMemcpyAsync(dcoef, coef.data(), (size_t)nts * sizeof(cplx), cudaMemcpyHostToDevice, st));
+  const cplx* Sm = c.S.get();
+  if (c.x2c()) {
+    cplx* S2 = (cplx*)c.scratch.get(SL_Q0_S, (size_t)nk * m2 * sizeof(cplx));
+    q0_x2c_overlap_kernel<<<grid_for((int64_t)nk * m2, 256), 256, 0, st>>>(c.S.get(), S2, nk, (int)d.nao);
+    GB_CHECK_LAUNCH();
+    Sm = S2;
+  }
+  const int64_t per_t = nmat * m2;
+  cplx* T = (cplx*)c.scratch.get(SL_Q0_T, (size_t)nts * per_t * sizeof(cplx));
+  cplx* D = (cplx*)c.scratch.get(SL_Q0_D, (size_t)nts * per_t * sizeof(cplx));
+  ZGemm a;  // T[t][sk] = S[sk] G[t][sk]
+  a.M = nso; a.N = nso; a.K = nso; a.nb1 = nts; a.nb2 = nmat;
+  a.A = dense(Sm, nso); a.A.bat.s2 = m2;
+  a.B = dense(G, nso); a.B.bat.s1 = per_t; a.B.bat.s2 = m2;
+  a.C.ptr = T; a.C.row = lin(nso); a.C.col = lin(1); a.C.bat.s1 = per_t; a.C.bat.s2 = m2;
+  zgemm_fp64(a, st);
+  q0_scale_kernel<<<grid_for((int64_t)nts * per_t, 256), 256, 0, st>>>(T, dcoef, nts, per_t);
+  GB_CHECK_LAUNCH();
+  ZGemm b;  // D[t][sk] = T[t][sk] S[sk]
+  b.M = nso; b.N = nso; b.K = nso; b.nb1 = nts; b.nb2 = nmat;
+  b.A = dense(T, nso); b.A.bat.s1 = per_t; b.A.bat.s2 = m2;
+  b.B = dense(Sm, nso); b.B.bat.s2 = m2;
+  b.C.ptr = D; b.C.row = lin(nso); b.C.col = lin(1); b.C.bat.s1 = per_t; b.C.bat.s2 = m2;
+  zgemm_fp64(b, st);
+  if (c.x2c()) {
+    q0_x2c_offdiag_kernel<<<grid_for((int64_t)nts * nmat * d.nao * d.nao, 256), 256, 0, st>>>(D, (int64_t)nts * nmat,
+                                                                                             (int)d.nao);
+    GB_CHECK_LAUNCH();
+  }
+  add_kernel<<<grid_for((int64_t)nts * per_t, 256), 256, 0, st>>>(Sigma, D, (int64_t)nts * per_t);
+  GB_CHECK_LAUNCH();
+}
+
 void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
   const gb200_dims& d = c.d;
   require(d.nts % 2 == 0, GB200_ERR_WRONG_GRID, "Number of tau points should be even!!!");
@@ -148,6 +290,7 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
   const int64_t g_t = (int64_t)ns * g_s;           // stride of tau in G
   const double pref = (d.ns == 2 || x2c) ? 1.0 : 2.0;  // gw_cpu_kernel.cpp:167
   cplx* Sigma_out = Sigma;
+  const cplx* G_in = G;
   const cplx* Gbar = G;  // the operand of Gbar(beta - tau, k): block (b,a) for two-component input
   if (x2c) {
     const int64_t n = (int64_t)nts * 4 * nk * nao2;
@@ -184,6 +327,11 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
   };
 
   float t_p0 = 0, t_w = 0, t_sig = 0;
+  if (c.q0_on) {
+    require(c.q_begin <= 0 && (c.q_end < 0 || c.q_end >= nk), GB200_ERR_INVALID,
+            "q0 correction: needs all q-points in one context (it extrapolates over q)");
+    c.eps_inv.alloc((size_t)nw_b * nk);
+  }
   // this context's share of the q loop (gw_cpu_kernel.cpp:45 distributes q over nodes the same way);
   // the partial Sigma is already divided by nk, so shards sum to the full self-energy
   const int q0 = std::max(0, c.q_begin);
@@ -256,6 +404,24 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
       m.B = dense(Pw, NQ); m.B.bat.s2 = (int64_t)NQ * NQ;
       m.C.ptr = aug; m.C.row = lin(NQ); m.C.col = lin(1); m.C.bat.s2 = (int64_t)NQ * NQ;
       zgemm_fp64(m, st);
+      if (c.q0_on) {
+        // head of P(i Omega_n, q) on the plane-wave G = 0 component: eps_inv[n][q] =
+        // conj(A_q) P(i Omega_n) A_q (aux_to_PW_00, mbpt_q0_utils_t.cpp:11-20)
+        cplx* y = (cplx*)c.scratch.get(SL_Q0_Y, (size_t)nw_b * NQ * sizeof(cplx));
+        const cplx* Aq = c.AqQ.get() + (int64_t)q * NQ;
+        ZGemm hy;  // y[n][Q] = sum_Q' P[n][Q][Q'] A_q[Q']
+        hy.M = NQ; hy.N = 1; hy.K = NQ; hy.nb2 = nw_b;
+        hy.A = dense(aug, NQ); hy.A.bat.s2 = (int64_t)NQ * NQ;
+        hy.B.ptr = Aq; hy.B.row = lin(1); hy.B.col = lin(0);
+        hy.C.ptr = y; hy.C.row = lin(1); hy.C.col = lin(0); hy.C.bat.s2 = NQ;
+        zgemm_fp64(hy, st);
+        ZGemm he;  // eps_inv[n][q] = sum_Q conj(A_q[Q]) y[n][Q]
+        he.M = 1; he.N = 1; he.K = NQ; he.nb2 = nw_b;
+        he.A.ptr = Aq; he.A.row = lin(0); he.A.col = lin(1); he.A.conj = true;
+        he.B.ptr = y; he.B.row = lin(1); he.B.col = lin(0); he.B.bat.s2 = NQ;
+        he.C.ptr = c.eps_inv.get() + q; he.C.row = lin(0); he.C.col = lin(0); he.C.bat.s2 = nk;
+        zgemm_fp64(he, st);
+      }
       ZGemm bt;  // W(tau) = sum_n Ttn_b[t][n] P(i Omega_n) -> stored in P0
       bt.M = nts; bt.N = (int64_t)NQ * NQ; bt.K = nw_b;
       bt.A = dense(c.Ttn_b.get(), nw_b);
@@ -320,6 +486,7 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
     x2c_unpack_sigma_kernel<<<grid_for(n, 256), 256, 0, st>>>(Sigma, Sigma_out, nts, nk, (int)nao);
     GB_CHECK_LAUNCH();
   }
+  if (c.q0_on) apply_q0(c, G_in, Sigma_out, st);
   if (se) {
     int e = split_check_error(c, st);
     require(e == 0, GB200_ERR_CUDA, "split contraction: tensor-core pipeline wait timed out (code " + std::to_string(e) + ")");

@@ -60,7 +60,7 @@ EXPORTED = [
     "gb200_dyson_find_mu", "gb200_dyson_compute_G", "gb200_dyson_electrons", "gb200_energy",
     "gb200_iteration_device", "gb200_last_timings", "gb200_set_split_engine", "gb200_set_integrals_device",
     "gb200_set_q_range", "gb200_dyson_solve_device", "gb200_energy_device", "gb200_stats_enable", "gb200_stats_read",
-    "gb200_hf_fock_noalloc",
+    "gb200_hf_fock_noalloc", "gb200_set_q0_correction",
 ]
 
 
@@ -114,6 +114,7 @@ def load(path: str | None = None):
     ll = ctypes.POINTER(ctypes.c_longlong)
     L.gb200_stats_read.argtypes = [vp, ll, ll, dp, dp]
     L.gb200_hf_fock_noalloc.argtypes = [ctypes.POINTER(Dims), vp, vp, vp, ctypes.c_double, vp, vp]
+    L.gb200_set_q0_correction.argtypes = [vp, vp, vp, ctypes.c_double]
     _lib = L
     return L
 
@@ -263,6 +264,17 @@ class Context:
         """Deliver stored pairs [pair_begin, pair_begin + pair_count) from device memory."""
         self._check(self._L.gb200_set_integrals_device(self._h, which, ctypes.c_void_p(V_ptr), pair_begin, pair_count,
                                                        ctypes.c_void_p(stream)))
+
+    def set_q0_correction(self, AqQ, q_abs, madelung: float):
+        """The "extrapolate" q -> 0 correction (AqQ [nk, NQ] complex, q_abs [nk]); AqQ=None turns it off."""
+        if AqQ is None:
+            self._check(self._L.gb200_set_q0_correction(self._h, None, None, 0.0))
+            return
+        A = _c128(AqQ)
+        q = np.ascontiguousarray(q_abs, dtype=np.float64)
+        if A.shape != (self.dims.nk, self.dims.NQ) or q.shape != (self.dims.nk,):
+            raise ValueError("AqQ must be [nk, NQ] and q_abs [nk]")
+        self._check(self._L.gb200_set_q0_correction(self._h, _ptr(A), _ptr(q), float(madelung)))
 
     def set_q_range(self, q_begin: int, q_end: int):
         self._check(self._L.gb200_set_q_range(self._h, q_begin, q_end))

@@ -101,6 +101,16 @@ int gb200_set_integrals_device(gb200_context* ctx, int which, const double* V_de
  * (the allreduce of :53-54).  Default: all q. */
 int gb200_set_q_range(gb200_context* ctx, int q_begin, int q_end);
 
+/* The "extrapolate" q -> 0 treatment of the GW self-energy (q0_treatment, common_defs.h;
+ * mbpt_q0_utils_t.cpp:11-178, call sites gw_cpu_kernel.cpp:58-64,267-270): with AqQ
+ * [nk][NQ] (complex, the AqQ dataset of AqQ.h5) and q_abs [nk] (|q|), every gw_sigma call
+ * collects eps_inv(i Omega_n, q) = conj(A_q) P(i Omega_n, q) A_q, extrapolates its real part to
+ * q -> 0 with a quadratic fit over the distinct |q| in (0, 1], takes it to tau, and adds
+ * -madelung eps_inv(tau) S G(tau) S to Sigma (S from gb200_dyson_set_hamiltonian; spinor
+ * blocks with S_aa for two-component input).  Needs the full q range in one context.
+ * AqQ = NULL switches the correction off. */
+int gb200_set_q0_correction(gb200_context* ctx, const double* AqQ, const double* q_abs, double madelung);
+
 /* Contraction precision (GB200_PREC_*) and, for GB200_PREC_SPLIT, the number
  * of INT8 slices per operand (2..8). */
 int gb200_set_precision(gb200_context* ctx, int mode, int slices);

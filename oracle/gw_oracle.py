@@ -210,7 +210,7 @@ def symmetrize_P0(P0, nk):
         P0[nts - it - 1] = P0[it]
 
 
-def eval_P_tilde(P0, Tnt_b, Ttn_b):
+def eval_P_tilde(P0, Tnt_b, Ttn_b, return_w=False):
     """tau -> i Omega, (I - P0)^-1 P0 per frequency, back to tau (gw_cpu_kernel.cpp:227-279).
 
     The reference inverts with Eigen's LDLT (:245-249), which reads only the
@@ -225,7 +225,59 @@ def eval_P_tilde(P0, Tnt_b, Ttn_b):
         temp = np.linalg.solve(hermitian_from_lower(I - Pw[n]), I)
         temp = 0.5 * (temp + np.conj(temp.T))
         Pw[n] = temp @ Pw[n]
-    return (Ttn_b @ Pw.reshape(Pw.shape[0], NQ * NQ)).reshape(nts, NQ, NQ)
+    Pt = (Ttn_b @ Pw.reshape(Pw.shape[0], NQ * NQ)).reshape(nts, NQ, NQ)
+    return (Pt, Pw) if return_w else Pt
+
+
+# ----------------------------------------------------------------------------
+# q -> 0 correction (mbpt_q0_utils_t.cpp, "extrapolate" treatment)
+# ----------------------------------------------------------------------------
+def q0_head(Pw, Aq):
+    """eps_inv[n] = conj(Aq) . P(i Omega_n) . Aq (aux_to_PW_00, mbpt_q0_utils_t.cpp:11-20)."""
+    return np.array([np.conj(Aq) @ Pw[n] @ Aq for n in range(Pw.shape[0])])
+
+
+def extrapolate_q0(X, q_abs, fit_order=2, q_max=1.0):
+    """q -> 0 limit of Re X(q): quadratic least-squares fit over the first occurrences of the
+    distinct |q| in (0, q_max], normal equations (extrapolate_q0 / filter_q_abs / polyfit,
+    mbpt_q0_utils_t.cpp:30-86)."""
+    seen, idx = set(), []
+    for i, qa in enumerate(q_abs):
+        if 0.0 < qa <= q_max and qa not in seen:
+            seen.add(qa)
+            idx.append(i)
+    x = np.array([q_abs[i] for i in idx])
+    y = np.array([np.real(X[i]) for i in idx])
+    A = np.vander(x, fit_order + 1, increasing=True)
+    c = np.linalg.solve(A.T @ A, A.T @ y)
+    return c[0]
+
+
+def q0_correction(eps_inv_wq, q_abs, Ttn_b, G, S, madelung, X2C=False):
+    """Delta Sigma(t) = -madelung eps_inv_q0(t) S G(t) S (GW_q0_correction / apply_q0_correction
+    and apply_q0_correction_2C, mbpt_q0_utils_t.cpp:88-178).  eps_inv_wq: [nw_b, nq]; the
+    extrapolated head is taken to tau with the bosonic-to-fermionic-tau transform."""
+    e_w = np.array([extrapolate_q0(eps_inv_wq[n], q_abs) for n in range(eps_inv_wq.shape[0])], dtype=np.complex128)
+    e_t = Ttn_b @ e_w
+    nts, ns, nk, nso, _ = G.shape
+    D = np.zeros_like(G)
+    if not X2C:
+        for t in range(nts):
+            for s in range(ns):
+                for k in range(nk):
+                    D[t, s, k] = -madelung * e_t[t] * (S[s, k] @ G[t, s, k] @ S[s, k])
+        return D
+    nao = nso // 2
+    for t in range(nts):
+        for k in range(nk):
+            Sa = S[0, k, :nao, :nao]
+            Gm = G[t, 0, k]
+            D[t, 0, k, :nao, :nao] = -madelung * e_t[t] * (Sa @ Gm[:nao, :nao] @ Sa)
+            D[t, 0, k, nao:, nao:] = -madelung * e_t[t] * (Sa @ Gm[nao:, nao:] @ Sa)
+            off = madelung * e_t[t] * (Sa @ Gm[:nao, nao:] @ Sa)
+            D[t, 0, k, :nao, nao:] = -off
+            D[t, 0, k, nao:, :nao] = -np.conj(off.T)
+    return D
 
 
 def selfenergy_contraction(Gq, v, P):
@@ -254,12 +306,15 @@ def eval_selfenergy(G, v, k1, k1mq, P, Sigma, ns, X2C=False):
             Sigma[t, is_, k1, a * nao:(a + 1) * nao, b * nao:(b + 1) * nao] -= selfenergy_contraction(Gq, v, P[t])
 
 
-def gw_solve(G, integrals, bz, Tnt_b, Ttn_b, ns, NQ, X2C=False, q_list=None, k_list=None, return_P=False):
+def gw_solve(G, integrals, bz, Tnt_b, Ttn_b, ns, NQ, X2C=False, q_list=None, k_list=None, return_P=False,
+             q0=None):
     """gw_cpu_kernel::solve for the no-symmetry case (gw_cpu_kernel.cpp:31-72,74-134).
 
     ``integrals.pair(k1, k2)`` returns V(k1,k2) [NQ, nao, nao].
     ``q_list``/``k_list`` restrict the work to a sample (CPU-baseline timing);
     with the defaults the full self-energy is returned, already divided by nk.
+    ``q0 = (AqQ [nq, NQ], q_abs [nq], madelung, S [ns, nk, nso, nso])`` adds the
+    "extrapolate" q -> 0 correction (gw_cpu_kernel.cpp:58-64,267-270).
     """
     nts = G.shape[0]
     if nts % 2 != 0:
@@ -267,6 +322,7 @@ def gw_solve(G, integrals, bz, Tnt_b, Ttn_b, ns, NQ, X2C=False, q_list=None, k_l
     nk = bz.nk
     Sigma = np.zeros_like(G)
     Ps = {}
+    eps_cols = {}
     qs = range(nk) if q_list is None else q_list
     ks = range(nk) if k_list is None else k_list
     for q in qs:
@@ -275,13 +331,21 @@ def gw_solve(G, integrals, bz, Tnt_b, Ttn_b, ns, NQ, X2C=False, q_list=None, k_l
             k1q = bz.k1_from_k2q(k1, q)
             eval_P0_tilde(G, integrals.pair(k1, k1q), k1, k1q, P0, ns, X2C)
         symmetrize_P0(P0, nk)
-        P = eval_P_tilde(P0, Tnt_b, Ttn_b)
+        if q0 is not None:
+            P, Pw = eval_P_tilde(P0, Tnt_b, Ttn_b, return_w=True)
+            eps_cols[q] = q0_head(Pw, q0[0][q])
+        else:
+            P = eval_P_tilde(P0, Tnt_b, Ttn_b)
         if return_P:
             Ps[q] = P
         for k1 in ks:
             k1mq = bz.k2_from_k1q(k1, q)
             eval_selfenergy(G, integrals.pair(k1, k1mq), k1, k1mq, P, Sigma, ns, X2C)
     Sigma /= nk
+    if q0 is not None:
+        AqQ, q_abs, madelung, S = q0
+        eps = np.stack([eps_cols[q] for q in range(nk)], axis=1)  # [nw_b, nq]
+        Sigma += q0_correction(eps, q_abs, Ttn_b, G, S, madelung, X2C)
     return (Sigma, Ps) if return_P else Sigma
 
 

@@ -264,3 +264,51 @@ def test_dyson_x2c_matches_oracle(gpu):
         e_gpu = c.energy(Gref, F1, sig)
     e_ref = O.compute_energy(Gref, F1, sig, H, g.Tnt_f, g.Ttn_beta, 1.0 / nk, X2C=True)
     np.testing.assert_allclose(e_gpu, e_ref, rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("x2c", [False, True])
+def test_gw_q0_correction_matches_oracle(gpu, x2c):
+    """The "extrapolate" q -> 0 correction (mbpt_q0_utils_t.cpp:11-178) on top of Sigma: scalar
+    and two-component input against the oracle at 1e-10."""
+    s = system("small")
+    nk, nao, NQ, g = s.nk, s.nao, s.NQ, s.grid
+    rng = np.random.default_rng(5)
+    A = rng.standard_normal((nk, NQ)) + 1j * rng.standard_normal((nk, NQ))
+    A /= np.linalg.norm(A, axis=1, keepdims=True)
+    q_abs = np.array([0.0, 0.21, 0.34, 0.52])
+    mad = 0.37
+    nso = 2 * nao if x2c else nao
+    ns = 1 if x2c else s.ns
+    if x2c:
+        G = np.zeros((g.nts, 1, nk, nso, nso), dtype=np.complex128)
+        G[:, 0, :, :nao, :nao] = s.G[:, 0]
+        G[:, 0, :, nao:, nao:] = 0.6 * s.G[:, 0]
+        X = rng.standard_normal((nk, nao, nao)) + 1j * rng.standard_normal((nk, nao, nao))
+        G[:, 0, :, :nao, nao:] = 0.05 * X
+        G[:, 0, :, nao:, :nao] = 0.03 * np.conj(np.swapaxes(X, -1, -2))
+    else:
+        G = s.G.copy()
+    b = rng.standard_normal((nk, nao, nao)) + 1j * rng.standard_normal((nk, nao, nao))
+    Saa = np.eye(nao) + 0.02 * (b + np.conj(np.swapaxes(b, -1, -2)))
+    S = np.zeros((ns, nk, nso, nso), dtype=np.complex128)
+    H = np.zeros_like(S)
+    for sp in range(ns):
+        S[sp, :, :nao, :nao] = Saa
+        H[sp, :, :nao, :nao] = s.F[0]
+        if x2c:
+            S[sp, :, nao:, nao:] = Saa
+            H[sp, :, nao:, nao:] = s.F[0]
+    want = O.gw_solve(G, O.HalfStoredIntegrals(s.V_half), O.NoSymBZ(s.mesh), g.Tnt_b, g.Ttn_b, ns, NQ, X2C=x2c,
+                      q0=(A, q_abs, mad, S))
+    with lib.Context(nk, nao, ns, NQ, g.nts, g.nw, g.nw_b, s.beta, nso=nso) as c:
+        kp, km = solvers.kq_maps(s.mesh)
+        c.set_kq_maps(kp, km)
+        c.set_grid(g.Tnt_f, g.Ttn_f, g.Tnt_b, g.Ttn_b, g.wsample_f)
+        c.set_integrals(s.V_half, lib.INTEGRALS_GW)
+        c.set_hamiltonian(H, S)
+        c.set_q0_correction(A, q_abs, mad)
+        got = c.gw_sigma(G)
+        c.set_q_range(0, 2)
+        with pytest.raises(lib.mbpt_kernel_error):
+            c.gw_sigma(G)
+    assert rel(got, want) < TOL

@@ -211,3 +211,36 @@ def read_integrals(dirpath: str, npairs: int | None = None):
             raise ValueError(f"integral files hold {store.shape[0]} k-pairs, {npairs} expected")
         store = store[:npairs]
     return np.ascontiguousarray(store), version
+
+
+def read_q0(path: str):
+    """AqQ.h5 of the "extrapolate" q -> 0 treatment (mbpt_q0_utils_t.h:18-36): returns
+    (AqQ [nq_stored, NQ] complex, q_abs [nq_stored], madelung)."""
+    f = H5File(path)
+    A = _complex(f.read("AqQ"))
+    q_abs = np.asarray(f.read("q_abs"), dtype=np.float64).reshape(-1)
+    try:
+        mad = float(np.asarray(f.read("madelung")))
+    except Exception:
+        mad = None
+    if A.shape[0] != q_abs.shape[0]:
+        raise ValueError("AqQ.h5: AqQ and q_abs disagree on the number of q-points")
+    return np.ascontiguousarray(A), q_abs, mad
+
+
+def q0_full_zone(AqQ_ibz, q_abs_ibz, ibz2bz_q, nq: int):
+    """Full-zone arrays for gb200_set_q0_correction from the irreducible ones: the irreducible
+    q-points keep their AqQ row and |q|, the others get |q| = 0, which excludes them from the
+    q -> 0 fit, so the fit uses the same points as the reference's loop over irreducible q."""
+    AqQ_ibz = np.asarray(AqQ_ibz)
+    ibz2bz_q = np.asarray(ibz2bz_q, dtype=np.int64)
+    if AqQ_ibz.shape[0] != len(ibz2bz_q):
+        raise ValueError(f"AqQ holds {AqQ_ibz.shape[0]} q-points, the symmetry tables {len(ibz2bz_q)} irreducible ones")
+    if len(ibz2bz_q) > 1 and (np.diff(ibz2bz_q) <= 0).any():
+        raise ValueError("irreducible q-points must be listed in increasing full-zone order")
+    A = np.zeros((nq, AqQ_ibz.shape[1]), dtype=np.complex128)
+    q = np.zeros(nq)
+    A[ibz2bz_q] = AqQ_ibz
+    q[ibz2bz_q] = np.asarray(q_abs_ibz)
+    return A, q
+

@@ -48,7 +48,7 @@ def make_context(system: System, device: int = 0, precision: int = lib.PREC_FP64
 
 
 def context_from_files(input_path: str, hf_integrals: str | None = None, gw_integrals: str | None = None,
-                       grid=None, beta: float | None = None, device: int = 0):
+                       grid=None, beta: float | None = None, device: int = 0, q0_file: str | None = None):
     """A context for a system written in green-mbpt's file format.
 
     input_path: input.h5 (parameters, Hamiltonian blocks, k-point symmetry); hf_integrals /
@@ -56,6 +56,8 @@ def context_from_files(input_path: str, hf_integrals: str | None = None, gw_inte
     Objects at irreducible k-points and irreducible k-pair integrals are expanded to the full
     zone on the host (inputs.KSymmetry).  `grid` (a grids.ChebyshevGrid or any object with
     Tnt_f, Ttn_f, Tnt_b, Ttn_b, wsample_f, nts, nw, nw_b) is needed for GW and the Dyson step.
+    q0_file: an AqQ.h5 switches on the "extrapolate" q -> 0 correction (irreducible q-points
+    of the input's q symmetry; the Madelung constant of the input).
     Returns (context, input dictionary).
     """
     from . import inputs
@@ -78,6 +80,12 @@ def context_from_files(input_path: str, hf_integrals: str | None = None, gw_inte
     if gw_integrals:
         store, _ = inputs.read_integrals(gw_integrals, npairs)
         ctx.set_integrals(sym.half_storage(store), lib.INTEGRALS_GW)
+    if q0_file:
+        from .h5lite import H5File
+        A, q_abs, _ = inputs.read_q0(q0_file)
+        ibz2bz_q = np.asarray(H5File(input_path).read("symmetry/q/ibz2bz"))
+        Af, qf = inputs.q0_full_zone(A, q_abs, ibz2bz_q, nk)
+        ctx.set_q0_correction(Af, qf, inp["madelung"])
     if "S_ibz" in inp:
         inp["S"] = sym.full_from_ibz(inp["S_ibz"])
     if "H_ibz" in inp:

@@ -79,3 +79,19 @@ def test_read_green_mbpt_files(case, name):
     assert inp["madelung"] == float(d["madelung"])
     assert version == str(d["version"].astype(str))
     assert lib.check_integral_version(version)
+
+
+def test_q0_full_zone_layout():
+    A = np.arange(6).reshape(3, 2) + 1j
+    A2, q2 = inputs.q0_full_zone(A, [0.0, 0.4, 0.7], [0, 2, 5], 6)
+    np.testing.assert_array_equal(A2[[0, 2, 5]], A)
+    np.testing.assert_array_equal(q2, [0.0, 0.0, 0.4, 0.0, 0.0, 0.7])
+    with pytest.raises(ValueError):
+        inputs.q0_full_zone(A, [0.0, 0.4, 0.7], [0, 5, 2], 6)
+
+
+@pytest.mark.skipif(not DATA, reason="GREEN_MBPT_TEST_DATA (green-mbpt's test/data) not given")
+def test_read_aqq_file():
+    A, q_abs, mad = inputs.read_q0(os.path.join(DATA, "GW", "df_hf_int", "AqQ.h5"))
+    assert A.shape == (q_abs.shape[0], 36) and q_abs[0] == 0.0 and (q_abs[1:] > 0).all()
+    assert mad is not None and mad > 0

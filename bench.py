@@ -237,15 +237,18 @@ def run_ours(args):
 
     def iteration():
         if ws == 1:
+            # the chemical-potential search starts from the previous iteration's mu, as the
+            # reference's dyson object does (its _mu persists across iterations, dyson.cpp:101-174)
             state["mu"], state["E"] = ctx.iteration_device(G.data_ptr(), S1.data_ptr(), St.data_ptr(), mad, nel, tol,
-                                                           0.0, stream=sptr)
+                                                           state["mu"], stream=sptr)
             return
         # q-sharded GW: partial self-energies are summed before the Dyson step
         dm.copy_(G[-1] * (-1.0 if s.ns == 2 else -2.0))
         ctx.hf_fock_device(dm.data_ptr(), Sdev.data_ptr(), mad, S1.data_ptr(), stream=sptr)
         ctx.gw_sigma_device(G.data_ptr(), St.data_ptr(), stream=sptr)
         shard.reduce_partial_sigma(St, dist)
-        state["mu"] = ctx.dyson_solve_device(S1.data_ptr(), St.data_ptr(), nel, tol, 0.0, G.data_ptr(), stream=sptr)
+        state["mu"] = ctx.dyson_solve_device(S1.data_ptr(), St.data_ptr(), nel, tol, state["mu"], G.data_ptr(),
+                                             stream=sptr)
         state["E"] = ctx.energy_device(G.data_ptr(), S1.data_ptr(), St.data_ptr(), stream=sptr)
 
     def step(ev=None):

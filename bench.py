@@ -295,7 +295,8 @@ def run_ours(args):
         comp_ms, tot_ms = float(t[0]), float(t[1])
     return s, ctx, dict(comp_ms=comp_ms, tot_ms=tot_ms, gw_ms=gw_ms, clocks=clk, launches=launches1 - launches0,
                         tc_n=tc_n, tc_ms=tc_ms, tc_fl=tc_fl, E=state["E"], mu=state["mu"],
-                        bytes_io=G0.numel() * 16, ws=ws, rank=rank, dist=dist, G0=G0, G=G, St=St, sptr=sptr)
+                        bytes_io=G0.numel() * 16, ws=ws, rank=rank, dist=dist, G0=G0, G=G, St=St, sptr=sptr,
+                        Gout=Gout)
 
 
 def fp64_sample(s, ctx, r, nq_sample):
@@ -361,6 +362,12 @@ def main_ours(args):
             "clocks": r["clocks"], "gpu_launches": r["launches"],
             "energies": {"E_1b": r["E"][0], "E_HF": r["E"][1], "E_corr": r["E"][2], "mu": r["mu"]} if r["E"] else None,
         }
+        # Chebyshev resolution of the new G (transformer_t::check_chebyshev's diagnostic): the
+        # grid is the same for the GPU path and the oracle, so this does not affect parity
+        try:
+            line["chebyshev_leakage_G"] = float(s.grid.leakage(r["Gout"].numpy()))
+        except Exception:
+            line["chebyshev_leakage_G"] = None
         if fp64_iter is not None:
             line["fp64_gpu"] = {"value": 1.0 / fp64_iter, "unit": UNIT,
                                 "estimate": f"FP64 GW timed on q-points [0,{args.fp64_q}) x {s.nk}, rest of the iteration measured"}

@@ -276,6 +276,31 @@ int gb200_gw_sigma_device(gb200_context* ctx, const double* G_dev, double* Sigma
   });
 }
 
+int gb200_gw_sigma_vjp(gb200_context* ctx, const double* G, const double* Sb, double* Gb) {
+  return guarded(ctx, [&](Context& c) {
+    require(G && Sb && Gb, GB200_ERR_INVALID, "gw_sigma_vjp: null pointer");
+    const size_t bytes = c.g_elems() * sizeof(cplx);
+    cplx* dG = (cplx*)c.scratch.get(SL_IO_G, bytes);
+    cplx* dSb = (cplx*)c.scratch.get(SL_IO_S, bytes);
+    cplx* dGb = (cplx*)c.scratch.get(SL_IO_S1, bytes);
+    HostIO::h2d(dG, G, bytes, c.stream);
+    HostIO::h2d(dSb, Sb, bytes, c.stream);
+    gw_sigma_vjp(c, dG, dSb, dGb, c.stream);
+    HostIO::d2h(Gb, dGb, bytes, c.stream);
+    GB_CUDA(cudaStreamSynchronize(c.stream));
+  });
+}
+
+int gb200_gw_sigma_vjp_device(gb200_context* ctx, const double* G_dev, const double* Sb_dev, double* Gb_dev,
+                              void* stream) {
+  return guarded(ctx, [&](Context& c) {
+    require(G_dev && Sb_dev && Gb_dev, GB200_ERR_INVALID, "gw_sigma_vjp_device: null pointer");
+    cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+    gw_sigma_vjp(c, reinterpret_cast<const cplx*>(G_dev), reinterpret_cast<const cplx*>(Sb_dev),
+                 reinterpret_cast<cplx*>(Gb_dev), st);
+  });
+}
+
 int gb200_hf_fock(gb200_context* ctx, const double* dm, const double* S, double madelung, double* F) {
   return guarded(ctx, [&](Context& c) {
     require(dm && S && F, GB200_ERR_INVALID, "hf_fock: null pointer");

@@ -60,7 +60,7 @@ EXPORTED = [
     "gb200_dyson_find_mu", "gb200_dyson_compute_G", "gb200_dyson_electrons", "gb200_energy",
     "gb200_iteration_device", "gb200_last_timings", "gb200_set_split_engine", "gb200_set_integrals_device",
     "gb200_set_q_range", "gb200_dyson_solve_device", "gb200_energy_device", "gb200_stats_enable", "gb200_stats_read",
-    "gb200_hf_fock_noalloc", "gb200_set_q0_correction",
+    "gb200_hf_fock_noalloc", "gb200_set_q0_correction", "gb200_gw_sigma_vjp", "gb200_gw_sigma_vjp_device",
 ]
 
 
@@ -96,6 +96,8 @@ def load(path: str | None = None):
     L.gb200_set_precision.argtypes = [vp, ip, ip]
     L.gb200_gw_sigma.argtypes = [vp, vp, vp]
     L.gb200_gw_sigma_device.argtypes = [vp, vp, vp, vp]
+    L.gb200_gw_sigma_vjp.argtypes = [vp, vp, vp, vp]
+    L.gb200_gw_sigma_vjp_device.argtypes = [vp, vp, vp, vp, vp]
     L.gb200_hf_fock.argtypes = [vp, vp, vp, ctypes.c_double, vp]
     L.gb200_hf_fock_device.argtypes = [vp, vp, vp, ctypes.c_double, vp, vp]
     L.gb200_dyson_set_hamiltonian.argtypes = [vp, vp, vp]
@@ -209,6 +211,13 @@ class Context:
         self._check(self._L.gb200_gw_sigma(self._h, _ptr(G), _ptr(out)))
         return out
 
+    def gw_sigma_vjp(self, G, Sigma_bar):
+        """Gb = d/dG of Re sum conj(Sigma_bar) Sigma(G) (FP64)."""
+        G, Sb = _c128(G), _c128(Sigma_bar)
+        out = np.empty(self.shape_G, dtype=np.complex128)
+        self._check(self._L.gb200_gw_sigma_vjp(self._h, _ptr(G), _ptr(Sb), _ptr(out)))
+        return out
+
     def hf_fock(self, dm, S, madelung=0.0):
         dm, S = _c128(dm), _c128(S)
         out = np.empty(self.shape_F, dtype=np.complex128)
@@ -246,6 +255,10 @@ class Context:
     def gw_sigma_device(self, G_ptr: int, Sigma_ptr: int, stream: int = 0):
         self._check(self._L.gb200_gw_sigma_device(self._h, ctypes.c_void_p(G_ptr), ctypes.c_void_p(Sigma_ptr),
                                                   ctypes.c_void_p(stream)))
+
+    def gw_sigma_vjp_device(self, G_ptr: int, Sb_ptr: int, Gb_ptr: int, stream: int = 0):
+        self._check(self._L.gb200_gw_sigma_vjp_device(self._h, ctypes.c_void_p(G_ptr), ctypes.c_void_p(Sb_ptr),
+                                                      ctypes.c_void_p(Gb_ptr), ctypes.c_void_p(stream)))
 
     def hf_fock_device(self, dm_ptr: int, S_ptr: int, madelung: float, F_ptr: int, stream: int = 0):
         self._check(self._L.gb200_hf_fock_device(self._h, ctypes.c_void_p(dm_ptr), ctypes.c_void_p(S_ptr),

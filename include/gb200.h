@@ -121,6 +121,16 @@ int gb200_set_precision(gb200_context* ctx, int mode, int slices);
 int gb200_gw_sigma(gb200_context* ctx, const double* G, double* Sigma);
 int gb200_gw_sigma_device(gb200_context* ctx, const double* G_dev, double* Sigma_dev, void* stream);
 
+/* Vector-Jacobian product of the GW self-energy with respect to G (FP64):
+ * Gb = d/dG of L = Re sum conj(Sb) Sigma(G), so that dL = Re sum conj(Gb) dG for every
+ * complex dG; G, Sb and Gb are [nts, ns, nk, nso, nso].  The reference computes no
+ * derivatives: this is the adjoint of gw_cpu_kernel::solve (gw_cpu_kernel.cpp:31-72), for
+ * gradients of GW functionals with respect to the Green's function.  Scalar (non-two-component)
+ * input without the q -> 0 correction; the forward of every q is recomputed in FP64. */
+int gb200_gw_sigma_vjp(gb200_context* ctx, const double* G, const double* Sb, double* Gb);
+int gb200_gw_sigma_vjp_device(gb200_context* ctx, const double* G_dev, const double* Sb_dev, double* Gb_dev,
+                              void* stream);
+
 /* Hartree-Fock Fock matrix F [ns, nk, nso, nso] from the density matrix dm
  * and overlap S (same shape).  Replaces hf_scalar_cpu_kernel::solve
  * (hf_cpu_kernels.cpp:25-146) and, for nso = 2 nao, hf_x2c_cpu_kernel::solve

@@ -349,6 +349,102 @@ def gw_solve(G, integrals, bz, Tnt_b, Ttn_b, ns, NQ, X2C=False, q_list=None, k_l
     return (Sigma, Ps) if return_P else Sigma
 
 
+def herm(X):
+    return 0.5 * (X + np.conj(np.swapaxes(X, -1, -2)))
+
+
+def hermitian_from_lower_adjoint(Ab):
+    """Adjoint (real inner product Re<a, b>) of X -> hermitian_from_lower(X)."""
+    n = Ab.shape[-1]
+    Xb = np.zeros_like(Ab)
+    low = np.tril_indices(n, -1)
+    Xb[low] = Ab[low] + np.conj(Ab.T[low])
+    Xb[np.diag_indices(n)] = np.real(np.diag(Ab))
+    return Xb
+
+
+def gw_vjp_G(G, integrals, bz, Tnt_b, Ttn_b, ns, NQ, Sigma_bar):
+    """Vector-Jacobian product of the GW self-energy (gw_solve, no X2C, no q0) with respect to G.
+
+    With L = Re sum conj(Sigma_bar) Sigma(G), returns Gbar such that dL = Re sum conj(Gbar) dG
+    for every complex perturbation dG (real and imaginary parts independent).  This is not a
+    restatement of the reference (which has no derivatives); it is the adjoint of the forward
+    restatement above, step by step, and is checked against central finite differences.
+    """
+    nts = G.shape[0]
+    nth = nts // 2
+    nk = bz.nk
+    pref = 1.0 if ns == 2 else 2.0
+    Gbar = np.zeros_like(G)
+    I = np.eye(NQ, dtype=np.complex128)
+    for q in range(nk):
+        # ---- forward of this q (recomputed) ----
+        P0 = np.zeros((nts, NQ, NQ), dtype=np.complex128)
+        for k1 in range(nk):
+            k1q = bz.k1_from_k2q(k1, q)
+            eval_P0_tilde(G, integrals.pair(k1, k1q), k1, k1q, P0, ns)
+        symmetrize_P0(P0, nk)
+        nwb = Tnt_b.shape[0]
+        Pw = (Tnt_b @ P0.reshape(nts, NQ * NQ)).reshape(nwb, NQ, NQ)
+        T = np.empty_like(Pw)
+        Th = np.empty_like(Pw)
+        Ptw = np.empty_like(Pw)
+        for n in range(nwb):
+            T[n] = np.linalg.solve(hermitian_from_lower(I - Pw[n]), I)
+            Th[n] = herm(T[n])
+            Ptw[n] = Th[n] @ Pw[n]
+        W = (Ttn_b @ Ptw.reshape(nwb, NQ * NQ)).reshape(nts, NQ, NQ)
+        # ---- Sigma = -(1/nk) sum_QQ' W_QQ' V^Q G V^Q'^H ----
+        Wbar = np.zeros_like(W)
+        for k1 in range(nk):
+            k1mq = bz.k2_from_k1q(k1, q)
+            v = integrals.pair(k1, k1mq)
+            vh = np.conj(np.swapaxes(v, -1, -2))
+            for t in range(nts):
+                for s_ in range(ns):
+                    Gq = G[t, s_, k1mq]
+                    Sb = Sigma_bar[t, s_, k1]
+                    # Gbar += -(1/nk) sum_QQ' conj(W_QQ') V^Q^H Sb V^Q'
+                    A = np.einsum("qim,ij->qmj", np.conj(v), Sb)           # (V^Q^H Sb)[m][j]
+                    Y = np.einsum("Qjn,qmj->qQmn", v, A)                   # (V^Q^H Sb V^Q')[m][n]
+                    Gbar[t, s_, k1mq] += -(1.0 / nk) * np.einsum("qQ,qQmn->mn", np.conj(W[t]), Y)
+                    # Wbar_QQ' += -(1/nk) tr(V^Q^H Sb V^Q' G^H)
+                    Wbar[t] += -(1.0 / nk) * np.einsum("qQmn,mn->qQ", Y, np.conj(Gq))
+        # ---- W = Ttn_b Ptw ----
+        Ptw_bar = (np.conj(Ttn_b).T @ Wbar.reshape(nts, NQ * NQ)).reshape(nwb, NQ, NQ)
+        Pw_bar = np.zeros_like(Pw)
+        for n in range(nwb):
+            Th_bar = Ptw_bar[n] @ np.conj(Pw[n].T)
+            Pw_bar[n] = np.conj(Th[n].T) @ Ptw_bar[n]
+            T_bar = herm(Th_bar)
+            TH = np.conj(T[n].T)
+            A_bar = -TH @ T_bar @ TH
+            Pw_bar[n] += -hermitian_from_lower_adjoint(A_bar)
+        # ---- Pw = Tnt_b P0;  P0 = symmetrize(P0h) ----
+        P0_bar = (np.conj(Tnt_b).T @ Pw_bar.reshape(nwb, NQ * NQ)).reshape(nts, NQ, NQ)
+        P0h_bar = np.zeros_like(P0_bar)
+        for t in range(nth):
+            P0h_bar[t] = herm(P0_bar[t] + P0_bar[nts - 1 - t]) / nk
+        # ---- P0h_QQ' = -pref sum_{k,s} tr(V^Q'^H Gb V^Q G1), Gb = G(beta - t, k), G1 = G(t, k + q) ----
+        for k1 in range(nk):
+            k1q = bz.k1_from_k2q(k1, q)
+            v = integrals.pair(k1, k1q)
+            vh = np.conj(np.swapaxes(v, -1, -2))
+            for t in range(nth):
+                tt = nts - 1 - t
+                for s_ in range(ns):
+                    Gb = G[tt, s_, k1]
+                    G1 = G[t, s_, k1q]
+                    Pb = P0h_bar[t]
+                    # Gb_bar = -pref sum_QQ' Pb_QQ' V^Q' G1^H V^Q^H
+                    X = np.einsum("Qrn,mn->Qrm", v, np.conj(G1))            # V^Q' G1^H
+                    Gbar[tt, s_, k1] += -pref * np.einsum("qQ,Qrm,qmp->rp", Pb, X, vh)
+                    # G1_bar = -pref sum_QQ' Pb_QQ' V^Q^H Gb^H V^Q'
+                    Z = np.einsum("qmp,rp->qmr", vh, np.conj(Gb))           # V^Q^H Gb^H
+                    Gbar[t, s_, k1q] += -pref * np.einsum("qQ,qmr,Qrn->mn", Pb, Z, v)
+    return Gbar
+
+
 # ----------------------------------------------------------------------------
 # Hartree-Fock (hf_solver.cpp, hf_cpu_kernels.cpp)
 # ----------------------------------------------------------------------------

@@ -276,7 +276,7 @@ int gb200_gw_sigma_device(gb200_context* ctx, const double* G_dev, double* Sigma
   });
 }
 
-int gb200_gw_sigma_vjp(gb200_context* ctx, const double* G, const double* Sb, double* Gb) {
+int gb200_gw_sigma_vjp(gb200_context* ctx, const double* G, const double* Sb, double* Gb, double* Vb) {
   return guarded(ctx, [&](Context& c) {
     require(G && Sb && Gb, GB200_ERR_INVALID, "gw_sigma_vjp: null pointer");
     const size_t bytes = c.g_elems() * sizeof(cplx);
@@ -285,19 +285,30 @@ int gb200_gw_sigma_vjp(gb200_context* ctx, const double* G, const double* Sb, do
     cplx* dGb = (cplx*)c.scratch.get(SL_IO_S1, bytes);
     HostIO::h2d(dG, G, bytes, c.stream);
     HostIO::h2d(dSb, Sb, bytes, c.stream);
-    gw_sigma_vjp(c, dG, dSb, dGb, c.stream);
+    const int64_t nk = c.d.nk, pe = c.pair_elems();
+    cplx* dVf = Vb ? (cplx*)c.scratch.get(SL_ADJ_VBF, (size_t)nk * nk * pe * sizeof(cplx)) : nullptr;
+    gw_sigma_vjp(c, dG, dSb, dGb, dVf, c.stream);
     HostIO::d2h(Gb, dGb, bytes, c.stream);
+    if (Vb) {
+      const size_t hb = (size_t)(nk * (nk + 1) / 2) * pe * sizeof(cplx);
+      cplx* dVh = (cplx*)c.scratch.get(SL_ADJ_VBH, hb);
+      fold_pair_gradient(c, dVf, dVh, c.stream);
+      HostIO::d2h(Vb, dVh, hb, c.stream);
+    }
     GB_CUDA(cudaStreamSynchronize(c.stream));
   });
 }
 
 int gb200_gw_sigma_vjp_device(gb200_context* ctx, const double* G_dev, const double* Sb_dev, double* Gb_dev,
-                              void* stream) {
+                              double* Vb_dev, void* stream) {
   return guarded(ctx, [&](Context& c) {
     require(G_dev && Sb_dev && Gb_dev, GB200_ERR_INVALID, "gw_sigma_vjp_device: null pointer");
     cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+    const int64_t nk = c.d.nk, pe = c.pair_elems();
+    cplx* dVf = Vb_dev ? (cplx*)c.scratch.get(SL_ADJ_VBF, (size_t)nk * nk * pe * sizeof(cplx)) : nullptr;
     gw_sigma_vjp(c, reinterpret_cast<const cplx*>(G_dev), reinterpret_cast<const cplx*>(Sb_dev),
-                 reinterpret_cast<cplx*>(Gb_dev), st);
+                 reinterpret_cast<cplx*>(Gb_dev), dVf, st);
+    if (Vb_dev) fold_pair_gradient(c, dVf, reinterpret_cast<cplx*>(Vb_dev), st);
   });
 }
 

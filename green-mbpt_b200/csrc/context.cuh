@@ -56,7 +56,8 @@ enum ScratchSlot {
   SL_HF_Y, SL_HF_U, SL_HF_DMT, SL_DY_SW, SL_DY_GW, SL_DY_X, SL_RED, SL_IO_G, SL_IO_S,
   SL_IO_S1, SL_IO_H, SL_DM, SL_PINV, SL_SPLIT0, SL_HF_TAB, SL_X2C_DM, SL_X2C_S, SL_X2C_F, SL_X2C_GAB, SL_X2C_GBA,
   SL_X2C_SIG, SL_Q0_Y, SL_Q0_T, SL_Q0_D, SL_Q0_E, SL_Q0_S, SL_ADJ_TH, SL_ADJ_PTW, SL_ADJ_W, SL_ADJ_WB,
-  SL_ADJ_PTWB, SL_ADJ_PWB, SL_ADJ_THB, SL_ADJ_XB, SL_ADJ_AB, SL_ADJ_P0B, SL_ADJ_P0HB, SL_ADJ_X3, SL_ADJ_TAB, SL_COUNT
+  SL_ADJ_PTWB, SL_ADJ_PWB, SL_ADJ_THB, SL_ADJ_XB, SL_ADJ_AB, SL_ADJ_P0B, SL_ADJ_P0HB, SL_ADJ_X3, SL_ADJ_TAB, SL_ADJ_TQ, SL_ADJ_VBF, SL_ADJ_VBH,
+  SL_COUNT
 };
 
 struct SplitEngine;
@@ -127,8 +128,11 @@ struct Context {
 void build_tables(Context& c);
 void build_hf_tables(Context& c);
 void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st);
-// Gb = d/dG of Re sum conj(Sb) Sigma(G) (FP64; no two-component input, no q -> 0 correction)
-void gw_sigma_vjp(Context& c, const cplx* G, const cplx* Sb, cplx* Gb, cudaStream_t st);
+// Gb = d/dG of Re sum conj(Sb) Sigma(G, V) (FP64; no two-component input, no q -> 0 correction);
+// with Vb non-null also d/dV on the full pair set [nk][nk][NQ][nao][nao] (zeroed here)
+void gw_sigma_vjp(Context& c, const cplx* G, const cplx* Sb, cplx* Gb, cplx* Vb, cudaStream_t st);
+// gradient of the half-stored integrals [nk(nk+1)/2][NQ][nao][nao] from the one of the full pair set
+void fold_pair_gradient(Context& c, const cplx* full, cplx* half, cudaStream_t st);
 // q -> 0 limit of the collected heads eps_inv[nw_b][nq] (mbpt_q0_utils_t.cpp:30-86), on the host
 cplx extrapolate_q0(const cplx* eps_n, const std::vector<double>& q_abs, int fit_order, double q_max);
 void hf_fock(Context& c, const cplx* dm, const cplx* S, double madelung, cplx* F, cudaStream_t st);

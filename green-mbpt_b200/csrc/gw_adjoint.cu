@@ -8,7 +8,9 @@
 //   W = Ttn_b herm(T) Pw,  T = hfl(I - Pw)^-1        -> Pw_bar (hfl: lower triangle + real diagonal)
 //   Pw = Tnt_b P0,  P0 = symmetrize(P0h)              -> P0h_bar
 //   P0h_QQ' = -pref sum tr(V^Q'^H Gbar V^Q G1)          -> Gb at G(beta - tau, k) and G(tau, k + q)
-// with the contractions ordered so that no NQ x NQ x nao^2 intermediate appears.
+// with the contractions ordered so that no NQ x NQ x nao^2 intermediate appears.  With Vb the
+// gradient with respect to the full pair set [nk][nk][NQ][nao][nao] is accumulated as well: V enters
+// Sigma through V(k, k - q) and P0 through V(k, k + q), each twice (V^Q and conj(V^Q')).
 #include <algorithm>
 #include <vector>
 
@@ -77,17 +79,38 @@ __global__ void adj_hfl_back_kernel(const cplx* Ab, cplx* Pwb, int64_t nmat, int
   }
 }
 
-}  // namespace
-
-namespace {
 // offsets of the (kk, s) blocks of a [kk][t][s][...] intermediate: tab[kk*ns + s] = kk*blk + s*pe
 __global__ void ks_table_kernel(int64_t* tab, int kbk, int ns, int64_t blk, int64_t pe) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < kbk * ns) tab[i] = (int64_t)(i / ns) * blk + (int64_t)(i % ns) * pe;
 }
+
+// Vb_half[p(k1,k2)] = Vb[k1][k2] + (k1 > k2 ? Vb[k2][k1]^H per Q : 0): the (k2, k1) block of the full
+// pair set is the per-Q conjugate transpose of the stored (k1, k2) block (scatter_pairs_kernel)
+__global__ void fold_pair_gradient_kernel(const cplx* full, cplx* half, int nk, int NQ, int nao) {
+  const int64_t m2 = (int64_t)nao * nao, pe = (int64_t)NQ * m2;
+  const int64_t total = (int64_t)nk * (nk + 1) / 2 * pe;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t idx = e / pe, r = e - idx * pe;
+    int64_t k1 = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+    while (k1 * (k1 + 1) / 2 > idx) --k1;
+    while ((k1 + 1) * (k1 + 2) / 2 <= idx) ++k1;
+    const int64_t k2 = idx - k1 * (k1 + 1) / 2;
+    const int64_t Q = r / m2, ij = r - Q * m2, i = ij / nao, j = ij % nao;
+    cplx g = full[(k1 * nk + k2) * pe + r];
+    if (k1 != k2) g = cadd(g, cconj(full[(k2 * nk + k1) * pe + Q * m2 + j * nao + i]));
+    half[e] = g;
+  }
+}
 }  // namespace
 
-void gw_sigma_vjp(Context& c, const cplx* G, const cplx* Sb, cplx* Gb, cudaStream_t st) {
+void fold_pair_gradient(Context& c, const cplx* full, cplx* half, cudaStream_t st) {
+  const int64_t total = (int64_t)c.d.nk * (c.d.nk + 1) / 2 * c.pair_elems();
+  fold_pair_gradient_kernel<<<grid_for(total, 256), 256, 0, st>>>(full, half, c.d.nk, c.d.NQ, c.d.nao);
+  GB_CHECK_LAUNCH();
+}
+
+void gw_sigma_vjp(Context& c, const cplx* G, const cplx* Sb, cplx* Gb, cplx* Vb, cudaStream_t st) {
   const gb200_dims& d = c.d;
   require(d.nts % 2 == 0, GB200_ERR_WRONG_GRID, "Number of tau points should be even!!!");
   require(c.have_kq && c.have_grid && c.have_V, GB200_ERR_STATE, "gw_sigma_vjp: k/q maps, grid and integrals must be set");
@@ -127,6 +150,13 @@ void gw_sigma_vjp(Context& c, const cplx* G, const cplx* Sb, cplx* Gb, cudaStrea
   cplx* X2 = buf(SL_Y2, kb * blk);
   cplx* X3 = buf(SL_ADJ_X3, kb * blk);
   int64_t* tab_ks = (int64_t*)c.scratch.get(SL_ADJ_TAB, (size_t)kb * ns * sizeof(int64_t));
+  // tab_tq[t*ns + s] = t*NQ^2: the (tau, spin) blocks of an [nts][NQ][NQ] matrix set
+  int64_t* tab_tq = (int64_t*)c.scratch.get(SL_ADJ_TQ, (size_t)nts * ns * sizeof(int64_t));
+  if (Vb) {
+    ks_table_kernel<<<(unsigned)((nts * ns + 255) / 256), 256, 0, st>>>(tab_tq, nts, ns, nq2, 0);
+    GB_CHECK_LAUNCH();
+    GB_CUDA(cudaMemsetAsync(Vb, 0, (size_t)nk * nk * pe * sizeof(cplx), st));
+  }
 
   for (int q = 0; q < nk; ++q) {
     // ---------------- forward P0(tau, q), FP64 (the contractions (a)-(c) of gw.cu) ----------
@@ -221,6 +251,42 @@ void gw_sigma_vjp(Context& c, const cplx* G, const cplx* Sb, cplx* Gb, cudaStrea
       gs.C.bat.tab0 = tGm; gs.C.bat.s1 = g_t; gs.C.bat.s2 = g_s;
       gs.alpha = cmk(-1.0 / nk, 0.0); gs.beta = cmk(1.0, 0.0);
       zgemm_fp64(gs, st);
+      if (Vb) {
+        ZGemm f;  // F[kk][t][s][Q][j][m] = sum_n Z[kk][t][Q][j][n] conj(G(t,s,k-q)[m][n])
+        f.M = (int64_t)NQ * nao; f.N = nao; f.K = nao;
+        f.nb0 = kbk; f.nb1 = nts; f.nb2 = ns;
+        f.A.ptr = X2; f.A.row = lin(nao); f.A.col = lin(1); f.A.bat.s0 = (int64_t)nts * pe; f.A.bat.s1 = pe;
+        f.B.ptr = G; f.B.row = lin(1); f.B.col = lin(nao); f.B.conj = true;
+        f.B.bat.tab0 = tGm; f.B.bat.s1 = g_t; f.B.bat.s2 = g_s;
+        f.C.ptr = X3; f.C.row = lin(nao); f.C.col = lin(1);
+        f.C.bat.s0 = blk; f.C.bat.s1 = (int64_t)ns * pe; f.C.bat.s2 = pe;
+        zgemm_fp64(f, st);
+        ZGemm v1;  // Vb(k,k-q)[Q][i][m] -= (1/nk) sum_{(t,s),j} Sb(t,s,k)[i][j] F[kk][t][s][Q][j][m]
+        v1.M = nao; v1.N = nao; v1.K = (int64_t)nts * ns * nao;
+        v1.nb0 = kbk; v1.nb1 = NQ;
+        v1.A.ptr = Sb + (int64_t)k0 * ge; v1.A.row = lin(nao); v1.A.col = two(nao, 1, g_s); v1.A.bat.s0 = ge;
+        v1.B.ptr = X3; v1.B.row = two(nao, nao, pe); v1.B.col = lin(1); v1.B.bat.s0 = blk; v1.B.bat.s1 = nao2;
+        v1.C.ptr = Vb; v1.C.row = lin(nao); v1.C.col = lin(1); v1.C.bat.tab0 = tVm; v1.C.bat.s1 = nao2;
+        v1.alpha = cmk(-1.0 / nk, 0.0); v1.beta = cmk(1.0, 0.0);
+        zgemm_fp64(v1, st);
+        ZGemm h;  // H[kk][t][s][Q][j][n] = sum_m conj(A1[kk][t][s][Q][m][j]) G(t,s,k-q)[m][n]
+        h.M = (int64_t)NQ * nao; h.N = nao; h.K = nao;
+        h.nb0 = kbk; h.nb1 = nts; h.nb2 = ns;
+        h.A.ptr = X1; h.A.row = two(nao, 1, nao2); h.A.col = lin(nao); h.A.conj = true;
+        h.A.bat.s0 = blk; h.A.bat.s1 = (int64_t)ns * pe; h.A.bat.s2 = pe;
+        h.B.ptr = G; h.B.row = lin(nao); h.B.col = lin(1); h.B.bat.tab0 = tGm; h.B.bat.s1 = g_t; h.B.bat.s2 = g_s;
+        h.C.ptr = X3; h.C.row = lin(nao); h.C.col = lin(1);
+        h.C.bat.s0 = blk; h.C.bat.s1 = (int64_t)ns * pe; h.C.bat.s2 = pe;
+        zgemm_fp64(h, st);
+        ZGemm v2;  // Vb(k,k-q)[Q'][(j,n)] -= (1/nk) sum_{(t,s),Q} W(t)[Q][Q'] H[kk][t][s][Q][(j,n)]
+        v2.M = NQ; v2.N = nao2; v2.K = (int64_t)nts * ns * NQ;
+        v2.nb0 = kbk;
+        v2.A.ptr = W; v2.A.row = lin(1); v2.A.col = twotab(NQ, NQ, tab_tq);
+        v2.B.ptr = X3; v2.B.row = lin(nao2); v2.B.col = lin(1); v2.B.bat.s0 = blk;
+        v2.C.ptr = Vb; v2.C.row = lin(nao2); v2.C.col = lin(1); v2.C.bat.tab0 = tVm;
+        v2.alpha = cmk(-1.0 / nk, 0.0); v2.beta = cmk(1.0, 0.0);
+        zgemm_fp64(v2, st);
+      }
       ZGemm ut;  // Ut[kk][t][s][Q'][m][j] = sum_n conj(G(t,s,k-q)[m][n]) V(k,k-q)[Q'][j][n]
       ut.M = nao; ut.N = (int64_t)NQ * nao; ut.K = nao;
       ut.nb0 = kbk; ut.nb1 = nts; ut.nb2 = ns;
@@ -337,6 +403,41 @@ void gw_sigma_vjp(Context& c, const cplx* G, const cplx* Sb, cplx* Gb, cudaStrea
       g1b.C.bat.tab0 = tGp; g1b.C.bat.s1 = g_t; g1b.C.bat.s2 = g_s;
       g1b.alpha = cmk(-pref, 0.0); g1b.beta = cmk(1.0, 0.0);
       zgemm_fp64(g1b, st);
+      if (Vb) {
+        ZGemm v3;  // Vb(k,k+q)[Q][p][m] -= pref sum_{(t,s),n} D[kk][t][s][Q][p][n] conj(G(t,s,k+q)[m][n])
+        v3.M = nao; v3.N = nao; v3.K = (int64_t)nth * ns * nao;
+        v3.nb0 = kbk; v3.nb1 = NQ;
+        v3.A.ptr = X3; v3.A.row = lin(nao); v3.A.col = two(nao, 1, pe); v3.A.bat.s0 = cblk; v3.A.bat.s1 = nao2;
+        v3.B.ptr = G; v3.B.row = two(nao, 1, g_s); v3.B.col = lin(nao); v3.B.conj = true; v3.B.bat.tab0 = tGp;
+        v3.C.ptr = Vb; v3.C.row = lin(nao); v3.C.col = lin(1); v3.C.bat.tab0 = tVp; v3.C.bat.s1 = nao2;
+        v3.alpha = cmk(-pref, 0.0); v3.beta = cmk(1.0, 0.0);
+        zgemm_fp64(v3, st);
+        ZGemm a;  // T1 recomputed: X1[kk][t][s][Q][p][n] = (V(k,k+q)^Q G(t,s,k+q))[p][n]
+        a.M = (int64_t)nth * ns * nao; a.N = (int64_t)NQ * nao; a.K = nao;
+        a.nb0 = kbk;
+        a.A.ptr = G; a.A.row = two(nao, 1, g_s); a.A.col = lin(nao); a.A.bat.tab0 = tGp;
+        a.B.ptr = V; a.B.row = lin(1); a.B.col = lin(nao); a.B.bat.tab0 = tVp;
+        a.C.ptr = X1; a.C.row = two(nao, 1, pe); a.C.col = lin(nao); a.C.bat.s0 = cblk;
+        zgemm_fp64(a, st);
+        ZGemm b;  // Bt recomputed: X2[kk][t][s][Q][r][n] = sum_p Gbar(nts-1-t,s,k)[r][p] T1[..][Q][p][n]
+        b.M = nao; b.N = (int64_t)NQ * nao; b.K = nao;
+        b.nb0 = kbk; b.nb1 = nth; b.nb2 = ns;
+        b.A = dense(G + (int64_t)(nts - 1) * g_t + (int64_t)k0 * ge, nao);
+        b.A.bat.s0 = ge; b.A.bat.s1 = -g_t; b.A.bat.s2 = g_s;
+        b.B.ptr = X1; b.B.row = lin(nao); b.B.col = two(nao, 1, nao2);
+        b.B.bat.s0 = cblk; b.B.bat.s1 = (int64_t)ns * pe; b.B.bat.s2 = pe;
+        b.C.ptr = X2; b.C.row = lin(nao); b.C.col = two(nao, 1, nao2);
+        b.C.bat.s0 = cblk; b.C.bat.s1 = (int64_t)ns * pe; b.C.bat.s2 = pe;
+        zgemm_fp64(b, st);
+        ZGemm v4;  // Vb(k,k+q)[Q'][(r,n)] -= pref sum_{(t,s),Q} conj(P0hb(t)[Q][Q']) Bt[kk][t][s][Q][(r,n)]
+        v4.M = NQ; v4.N = nao2; v4.K = (int64_t)nth * ns * NQ;
+        v4.nb0 = kbk;
+        v4.A.ptr = P0hb; v4.A.row = lin(1); v4.A.col = twotab(NQ, NQ, tab_tq); v4.A.conj = true;
+        v4.B.ptr = X2; v4.B.row = lin(nao2); v4.B.col = lin(1); v4.B.bat.s0 = cblk;
+        v4.C.ptr = Vb; v4.C.row = lin(nao2); v4.C.col = lin(1); v4.C.bat.tab0 = tVp;
+        v4.alpha = cmk(-pref, 0.0); v4.beta = cmk(1.0, 0.0);
+        zgemm_fp64(v4, st);
+      }
     }
   }
 }

@@ -96,8 +96,8 @@ def load(path: str | None = None):
     L.gb200_set_precision.argtypes = [vp, ip, ip]
     L.gb200_gw_sigma.argtypes = [vp, vp, vp]
     L.gb200_gw_sigma_device.argtypes = [vp, vp, vp, vp]
-    L.gb200_gw_sigma_vjp.argtypes = [vp, vp, vp, vp]
-    L.gb200_gw_sigma_vjp_device.argtypes = [vp, vp, vp, vp, vp]
+    L.gb200_gw_sigma_vjp.argtypes = [vp, vp, vp, vp, vp]
+    L.gb200_gw_sigma_vjp_device.argtypes = [vp, vp, vp, vp, vp, vp]
     L.gb200_hf_fock.argtypes = [vp, vp, vp, ctypes.c_double, vp]
     L.gb200_hf_fock_device.argtypes = [vp, vp, vp, ctypes.c_double, vp, vp]
     L.gb200_dyson_set_hamiltonian.argtypes = [vp, vp, vp]
@@ -211,12 +211,16 @@ class Context:
         self._check(self._L.gb200_gw_sigma(self._h, _ptr(G), _ptr(out)))
         return out
 
-    def gw_sigma_vjp(self, G, Sigma_bar):
-        """Gb = d/dG of Re sum conj(Sigma_bar) Sigma(G) (FP64)."""
+    def gw_sigma_vjp(self, G, Sigma_bar, with_V: bool = False):
+        """Gb = d/dG of Re sum conj(Sigma_bar) Sigma(G, V) (FP64); with_V also returns Vb, the
+        gradient with respect to the half-stored integrals: (Gb, Vb)."""
         G, Sb = _c128(G), _c128(Sigma_bar)
         out = np.empty(self.shape_G, dtype=np.complex128)
-        self._check(self._L.gb200_gw_sigma_vjp(self._h, _ptr(G), _ptr(Sb), _ptr(out)))
-        return out
+        d = self.dims
+        Vb = np.empty((d.nk * (d.nk + 1) // 2, d.NQ, d.nao, d.nao), dtype=np.complex128) if with_V else None
+        self._check(self._L.gb200_gw_sigma_vjp(self._h, _ptr(G), _ptr(Sb), _ptr(out),
+                                               _ptr(Vb) if with_V else None))
+        return (out, Vb) if with_V else out
 
     def hf_fock(self, dm, S, madelung=0.0):
         dm, S = _c128(dm), _c128(S)
@@ -256,9 +260,10 @@ class Context:
         self._check(self._L.gb200_gw_sigma_device(self._h, ctypes.c_void_p(G_ptr), ctypes.c_void_p(Sigma_ptr),
                                                   ctypes.c_void_p(stream)))
 
-    def gw_sigma_vjp_device(self, G_ptr: int, Sb_ptr: int, Gb_ptr: int, stream: int = 0):
+    def gw_sigma_vjp_device(self, G_ptr: int, Sb_ptr: int, Gb_ptr: int, Vb_ptr: int = 0, stream: int = 0):
         self._check(self._L.gb200_gw_sigma_vjp_device(self._h, ctypes.c_void_p(G_ptr), ctypes.c_void_p(Sb_ptr),
-                                                      ctypes.c_void_p(Gb_ptr), ctypes.c_void_p(stream)))
+                                                      ctypes.c_void_p(Gb_ptr), ctypes.c_void_p(Vb_ptr or None),
+                                                      ctypes.c_void_p(stream)))
 
     def hf_fock_device(self, dm_ptr: int, S_ptr: int, madelung: float, F_ptr: int, stream: int = 0):
         self._check(self._L.gb200_hf_fock_device(self._h, ctypes.c_void_p(dm_ptr), ctypes.c_void_p(S_ptr),

@@ -121,15 +121,17 @@ int gb200_set_precision(gb200_context* ctx, int mode, int slices);
 int gb200_gw_sigma(gb200_context* ctx, const double* G, double* Sigma);
 int gb200_gw_sigma_device(gb200_context* ctx, const double* G_dev, double* Sigma_dev, void* stream);
 
-/* Vector-Jacobian product of the GW self-energy with respect to G (FP64):
- * Gb = d/dG of L = Re sum conj(Sb) Sigma(G), so that dL = Re sum conj(Gb) dG for every
- * complex dG; G, Sb and Gb are [nts, ns, nk, nso, nso].  The reference computes no
- * derivatives: this is the adjoint of gw_cpu_kernel::solve (gw_cpu_kernel.cpp:31-72), for
- * gradients of GW functionals with respect to the Green's function.  Scalar (non-two-component)
- * input without the q -> 0 correction; the forward of every q is recomputed in FP64. */
-int gb200_gw_sigma_vjp(gb200_context* ctx, const double* G, const double* Sb, double* Gb);
+/* Vector-Jacobian product of the GW self-energy (FP64).  With L = Re sum conj(Sb) Sigma(G, V):
+ * Gb = dL/dG [nts, ns, nk, nso, nso] and, when Vb is not NULL, Vb = dL/dV for the half-stored GW
+ * integrals [nk(nk+1)/2, NQ, nao, nao] (the layout gb200_set_integrals takes), so that
+ * dL = Re sum conj(Gb) dG + Re sum conj(Vb) dV for all complex dG, dV.  The reference computes
+ * no derivatives: this is the adjoint of gw_cpu_kernel::solve (gw_cpu_kernel.cpp:31-72), for
+ * gradients of GW functionals.  Scalar (non-two-component) input without the q -> 0 correction;
+ * P0 and W of every q are recomputed in FP64 rather than stored.  Needs one full-pair-set
+ * accumulator (nk^2 NQ nao^2 complex) on the device when Vb is requested. */
+int gb200_gw_sigma_vjp(gb200_context* ctx, const double* G, const double* Sb, double* Gb, double* Vb);
 int gb200_gw_sigma_vjp_device(gb200_context* ctx, const double* G_dev, const double* Sb_dev, double* Gb_dev,
-                              void* stream);
+                              double* Vb_dev, void* stream);
 
 /* Hartree-Fock Fock matrix F [ns, nk, nso, nso] from the density matrix dm
  * and overlap S (same shape).  Replaces hf_scalar_cpu_kernel::solve

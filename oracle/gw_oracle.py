@@ -371,11 +371,39 @@ def gw_vjp_G(G, integrals, bz, Tnt_b, Ttn_b, ns, NQ, Sigma_bar):
     restatement of the reference (which has no derivatives); it is the adjoint of the forward
     restatement above, step by step, and is checked against central finite differences.
     """
+    return gw_vjp(G, integrals, bz, Tnt_b, Ttn_b, ns, NQ, Sigma_bar, with_V=False)[0]
+
+
+def fold_pair_gradient(Vbar_full):
+    """Gradient with respect to the half-stored integrals [nk(nk+1)/2, NQ, nao, nao] from the one of
+    the full pair set [nk, nk, NQ, nao, nao]: the (k2, k1) block, k1 > k2, is the per-Q conjugate
+    transpose of the stored (k1, k2) block (HalfStoredIntegrals.pair), so its gradient enters the
+    stored block conjugate-transposed."""
+    nk = Vbar_full.shape[0]
+    out = np.zeros((nk * (nk + 1) // 2,) + Vbar_full.shape[2:], dtype=np.complex128)
+    for k1 in range(nk):
+        for k2 in range(k1 + 1):
+            g = Vbar_full[k1, k2].copy()
+            if k1 != k2:
+                g += np.conj(np.swapaxes(Vbar_full[k2, k1], -1, -2))
+            out[pair_index(k1, k2)] = g
+    return out
+
+
+def gw_vjp(G, integrals, bz, Tnt_b, Ttn_b, ns, NQ, Sigma_bar, with_V=True):
+    """Vector-Jacobian product of the GW self-energy with respect to G and to the half-stored
+    integrals: returns (Gbar, Vbar_half or None), dL = Re sum conj(Gbar) dG + Re sum conj(Vbar) dV
+    for L = Re sum conj(Sigma_bar) Sigma(G, V).  V enters Sigma through the pair V(k, k - q) twice
+    (V^Q and conj(V^Q')) and P0 through the pair V(k, k + q) twice, each one a term below."""
     nts = G.shape[0]
     nth = nts // 2
     nk = bz.nk
     pref = 1.0 if ns == 2 else 2.0
     Gbar = np.zeros_like(G)
+    Vbar = None
+    if with_V:
+        nao = G.shape[-1]
+        Vbar = np.zeros((nk, nk, NQ, nao, nao), dtype=np.complex128)
     I = np.eye(NQ, dtype=np.complex128)
     for q in range(nk):
         # ---- forward of this q (recomputed) ----
@@ -410,6 +438,13 @@ def gw_vjp_G(G, integrals, bz, Tnt_b, Ttn_b, ns, NQ, Sigma_bar):
                     Gbar[t, s_, k1mq] += -(1.0 / nk) * np.einsum("qQ,qQmn->mn", np.conj(W[t]), Y)
                     # Wbar_QQ' += -(1/nk) tr(V^Q^H Sb V^Q' G^H)
                     Wbar[t] += -(1.0 / nk) * np.einsum("qQmn,mn->qQ", Y, np.conj(Gq))
+                    if with_V:
+                        # Vbar^Q += -(1/nk) Sb sum_Q' conj(W_QQ') V^Q' G^H
+                        F = np.einsum("qQ,Qjn,mn->qjm", np.conj(W[t]), v, np.conj(Gq))
+                        Vbar[k1, k1mq] += -(1.0 / nk) * np.einsum("ij,qjm->qim", Sb, F)
+                        # Vbar^Q' += -(1/nk) sum_Q W_QQ' Sb^H V^Q G
+                        H = np.einsum("ij,qim,mn->qjn", np.conj(Sb), v, Gq)
+                        Vbar[k1, k1mq] += -(1.0 / nk) * np.einsum("qQ,qjn->Qjn", W[t], H)
         # ---- W = Ttn_b Ptw ----
         Ptw_bar = (np.conj(Ttn_b).T @ Wbar.reshape(nts, NQ * NQ)).reshape(nwb, NQ, NQ)
         Pw_bar = np.zeros_like(Pw)
@@ -442,7 +477,14 @@ def gw_vjp_G(G, integrals, bz, Tnt_b, Ttn_b, ns, NQ, Sigma_bar):
                     # G1_bar = -pref sum_QQ' Pb_QQ' V^Q^H Gb^H V^Q'
                     Z = np.einsum("qmp,rp->qmr", vh, np.conj(Gb))           # V^Q^H Gb^H
                     Gbar[t, s_, k1q] += -pref * np.einsum("qQ,qmr,Qrn->mn", Pb, Z, v)
-    return Gbar
+                    if with_V:
+                        # Vbar^Q += -pref Gb^H R^Q G1^H, R^Q = sum_Q' Pb_QQ' V^Q'
+                        R = np.einsum("qQ,Qrn->qrn", Pb, v)
+                        Vbar[k1, k1q] += -pref * np.einsum("rp,qrn,mn->qpm", np.conj(Gb), R, np.conj(G1))
+                        # Vbar^Q' += -pref sum_Q conj(Pb_QQ') Gb V^Q G1
+                        Bt = np.einsum("rp,qpm,mn->qrn", Gb, v, G1)
+                        Vbar[k1, k1q] += -pref * np.einsum("qQ,qrn->Qrn", np.conj(Pb), Bt)
+    return Gbar, (fold_pair_gradient(Vbar) if with_V else None)
 
 
 # ----------------------------------------------------------------------------

@@ -31,6 +31,46 @@ def test_gw_vjp_matches_oracle(gpu, name):
     assert rel(Gb, ref) < TOL
 
 
+@pytest.mark.parametrize("name", ["small", "small_ns2"])
+def test_gw_vjp_V_matches_oracle(gpu, name):
+    s = system(name)
+    g = s.grid
+    Sb = _cotangent(s.G.shape, 6)
+    Gref, Vref = O.gw_vjp(s.G, O.HalfStoredIntegrals(s.V_half), O.NoSymBZ(s.mesh), g.Tnt_b, g.Ttn_b, s.ns, s.NQ, Sb)
+    with solvers.make_context(s) as c:
+        Gb, Vb = c.gw_sigma_vjp(s.G, Sb, with_V=True)
+    assert rel(Gb, Gref) < TOL
+    assert rel(Vb, Vref) < TOL
+
+
+def test_gw_vjp_c4_finite_differences(gpu):
+    """At the differentiable-step size (nk=27, nao=20, naux=100, ntau=80) the adjoint against central
+    finite differences of the GPU forward (step 1e-6) along random directions in G and in V."""
+    s = system("c4")
+    Sb = _cotangent(s.G.shape, 7)
+    rng = np.random.default_rng(8)
+    h = 1e-6
+    with solvers.make_context(s) as c:
+        Gb, Vb = c.gw_sigma_vjp(s.G, Sb, with_V=True)
+
+        def loss_G(G):
+            return np.real(np.vdot(Sb, c.gw_sigma(G)))
+
+        E = _cotangent(s.G.shape, 9)
+        fd = (loss_G(s.G + h * E) - loss_G(s.G - h * E)) / (2 * h)
+        an = np.real(np.vdot(Gb, E))
+        assert abs(fd - an) <= 1e-6 * abs(fd)
+
+        def loss_V(V):
+            c.set_integrals(V, lib.INTEGRALS_GW)
+            return np.real(np.vdot(Sb, c.gw_sigma(s.G)))
+
+        EV = rng.standard_normal(s.V_half.shape) + 1j * rng.standard_normal(s.V_half.shape)
+        fd = (loss_V(s.V_half + h * EV) - loss_V(s.V_half - h * EV)) / (2 * h)
+        an = np.real(np.vdot(Vb, EV))
+        assert abs(fd - an) <= 1e-6 * abs(fd)
+
+
 def test_gw_vjp_linearity(gpu):
     """Sigma[G] is not complex-analytic (P0 is hermitized), so its adjoint is linear in the
     cotangent over the reals: Gb(a Sb1 + Sb2) = a Gb(Sb1) + Gb(Sb2) for real a."""
@@ -65,3 +105,20 @@ def test_vjp_rejects_q0_correction(gpu):
         c.set_q0_correction(np.ones((s.nk, s.NQ), dtype=np.complex128), np.linspace(0.1, 1.0, s.nk), 0.1)
         with pytest.raises(lib.mbpt_kernel_error):
             c.gw_sigma_vjp(s.G, _cotangent(s.G.shape))
+
+
+def test_autograd_gradient_V(gpu):
+    torch = pytest.importorskip("torch")
+    from gb200 import autograd
+    s = system("small_ns2")
+    Sb = _cotangent(s.G.shape, 10)
+    with solvers.make_context(s) as c:
+        G = torch.tensor(s.G, dtype=torch.complex128, device="cuda", requires_grad=True)
+        V = torch.tensor(s.V_half, dtype=torch.complex128, device="cuda", requires_grad=True)
+        Sigma = autograd.gw_sigma(c, G, V)
+        loss = torch.real(torch.sum(torch.conj(torch.tensor(Sb, device="cuda")) * Sigma))
+        loss.backward()
+        torch.cuda.synchronize()
+        Gb, Vb = c.gw_sigma_vjp(s.G, Sb, with_V=True)
+        assert rel(G.grad.cpu().numpy(), Gb) < 1e-13
+        assert rel(V.grad.cpu().numpy(), Vb) < 1e-13

@@ -51,6 +51,7 @@ WORKLOADS = {
     "c1": "c1: nk=64 (4x4x4), nao=26, naux=150, ns=2, ntau=100, beta=100, eps~U[-2,2]",
     "c0": "c0: nk=8 (2x2x2), nao=10, naux=40, ns=1, ntau=60, beta=100, eps~U[-2,2]",
     "c2k2": "c2k2: c2's shapes (nao=40, naux=250, ntau=120, nw=120) on a 2x1x1 mesh (nk=2): profiling case",
+    "c4": "c4: nk=27 (3x3x3), nao=20, naux=100, ns=1, ntau=80, beta=100, eps~U[-2,2]: differentiable step",
 }
 
 
@@ -410,6 +411,58 @@ def main_gw_profile(args):
     ctx.close()
 
 
+def main_newton(args):
+    """--newton N: the differentiable GW step (FP64).  Times the self-energy, its vector-Jacobian
+    product with respect to G and to G and V (CUDA events), then runs N plain iterations and N
+    Newton-Krylov steps from the same start (the non-interacting G, mu searched every iteration) and
+    prints their residual histories |Phi(G) - G|, map evaluations and device-synchronised times."""
+    import torch
+
+    from gb200 import newton, solvers, synth
+
+    torch.cuda.set_device(0)
+    s = synth.make_config(args.config, seed=args.seed)
+    ctx = solvers.make_context(s)
+    G = torch.from_numpy(s.G).cuda()
+    Sig, Sb = torch.empty_like(G), torch.randn_like(G)
+    Gb = torch.empty_like(G)
+    Vb = torch.empty((s.V_half.shape), dtype=torch.complex128, device="cuda")
+
+    def timed(fn, n):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(n):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / n
+
+    leg = 0x1  # the library call shares torch's default stream
+    t_fwd = timed(lambda: ctx.gw_sigma_device(G.data_ptr(), Sig.data_ptr(), stream=leg), 3)
+    t_vjp = timed(lambda: ctx.gw_sigma_vjp_device(G.data_ptr(), Sb.data_ptr(), Gb.data_ptr(), 0, stream=leg), 2)
+    t_vjp_v = timed(lambda: ctx.gw_sigma_vjp_device(G.data_ptr(), Sb.data_ptr(), Gb.data_ptr(), Vb.data_ptr(),
+                                                   stream=leg), 2)
+    it = newton.DeviceIteration(ctx, G, nel=s.nel_from_G0(), mu=0.0, tol=1e-12)
+    atol = 1e-11 * (1.0 + float(torch.linalg.norm(G)))  # about the FP64 floor of |Phi(G) - G|
+    out = {"workload": WORKLOADS[args.config], "precision": "FP64", "gw_sigma_ms": t_fwd,
+           "vjp_G_ms": t_vjp, "vjp_G_V_ms": t_vjp_v}
+    for name, run in (("plain", lambda: newton.plain_iteration(it, G, args.newton)),
+                      ("newton_krylov", lambda: newton.newton_krylov(it, G, args.newton, maxiter=30,
+                                                                      atol=atol))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        calls0 = it.calls
+        _, h = run()
+        torch.cuda.synchronize()
+        out[name] = {"steps": args.newton, "residual": h.residual, "map_evaluations": it.calls - calls0,
+                     "krylov_matvecs": h.krylov, "seconds": time.perf_counter() - t0}
+    print(json.dumps(out), flush=True)
+    ctx.close()
+
+
 def main_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -449,8 +502,11 @@ def parse(argv=None):
     ap.add_argument("--no-fp64-sample", action="store_true")
     ap.add_argument("--gw-q", dest="gw_q", type=int, default=0,
                     help="profiling case: time only the GW self-energy over q-points [0, GW_Q)")
+    ap.add_argument("--newton", type=int, default=0,
+                    help="differentiable-step case (--config c4): adjoint timings, then N plain and N "
+                         "Newton-Krylov self-consistency steps from the same start")
     a = ap.parse_args(argv)
-    if a.warmup < 3 and not a.gw_q:
+    if a.warmup < 3 and not (a.gw_q or a.newton):
         ap.error("at least 3 warm-up steps")
     return a
 
@@ -461,5 +517,7 @@ if __name__ == "__main__":
         main_reference(args)
     elif args.gw_q:
         main_gw_profile(args)
+    elif args.newton:
+        main_newton(args)
     else:
         main_ours(args)

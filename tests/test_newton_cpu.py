@@ -1,0 +1,59 @@
+"""Newton-Krylov self-consistency (gb200.newton) on the CPU: GMRES on a real-linear operator, and
+Newton-Krylov against the plain iteration on the oracle's iteration map (HF, GW, Dyson at fixed mu)."""
+import numpy as np
+import pytest
+import torch
+
+import gw_oracle as O
+from gb200 import newton
+from _systems import system
+
+
+def test_gmres_real_linear_operator():
+    rng = np.random.default_rng(0)
+    n = 40
+    M = torch.from_numpy(np.eye(n) * 3 + 0.2 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))))
+    N = torch.from_numpy(0.1 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))))
+
+    def A(x):  # real-linear, not complex-linear
+        return M @ x + N @ torch.conj(x)
+
+    xt = torch.from_numpy(rng.standard_normal(n) + 1j * rng.standard_normal(n))
+    b = A(xt)
+    x, res, used = newton.gmres(A, b, rtol=1e-12, restart=25, maxiter=200)
+    assert torch.linalg.norm(x - xt) <= 1e-9 * torch.linalg.norm(xt)
+    assert used <= 200
+
+
+def _oracle_phi(s, mu=0.0):
+    g = s.grid
+    integ, bz = O.HalfStoredIntegrals(s.V_half), O.NoSymBZ(s.mesh)
+
+    def phi(G):
+        Gn = G.numpy()
+        dm = O.hf_density(Gn, s.ns)
+        F = O.hf_scalar(dm, s.S, 0.0, integ.pair, lambda X, k: X[k], s.nk, lambda ik: ik, s.NQ)
+        sig = O.gw_solve(Gn, integ, bz, g.Tnt_b, g.Ttn_b, s.ns, s.NQ)
+        return torch.from_numpy(O.compute_G(F, sig, s.F, s.S, mu, g.Tnt_f, g.Ttn_f, g.wsample_f))
+    return phi
+
+
+@pytest.mark.parametrize("name", ["small", "small_ns2"])
+def test_newton_krylov_converges_quadratically(name):
+    s = system(name)
+    phi = _oracle_phi(s)
+    G0 = torch.from_numpy(s.G.copy())
+    Gn, hist = newton.newton_krylov(phi, G0, steps=6, atol=1e-12)
+    r = hist.residual
+    assert r[-1] < 1e-11
+    # superlinear: once below 1e-2 each Newton step at least squares the relative reduction
+    big = [x for x in r[1:] if 1e-9 < x < 1e-2]
+    for a, b in zip(big, big[1:]):
+        assert b < 10 * a * a + 1e-12
+    # the plain iteration reaches the same fixed point, with more steps
+    Gp, hp = newton.plain_iteration(phi, G0, 60)
+    assert hp.residual[-1] < 1e-10
+    assert float(torch.abs(Gn - Gp).max()) < 1e-9
+    # and, with the same number of map evaluations, is still far from it
+    _, hq = newton.plain_iteration(phi, G0, 8)
+    assert hq.residual[-1] > 1e3 * r[-1]

@@ -458,8 +458,8 @@ def main_newton(args):
         _, h = run()
         torch.cuda.synchronize()
         out[name] = {"steps": args.newton, "residual": h.residual, "map_evaluations": it.calls - calls0,
-                     "krylov_matvecs": h.krylov, "seconds": time.perf_counter() - t0}
-    print(json.dumps(out), flush=True)
+                     "krylov_matvecs": h.krylov, "seconds": time.perf_counter() - t0, "mu": it.last_mu}
+        print(json.dumps(out), flush=True)  # one line per stage, the last one complete
     ctx.close()
 
 

@@ -57,3 +57,27 @@ def test_newton_krylov_converges_quadratically(name):
     # and, with the same number of map evaluations, is still far from it
     _, hq = newton.plain_iteration(phi, G0, 8)
     assert hq.residual[-1] > 1e3 * r[-1]
+
+
+def test_newton_krylov_with_mu_search_where_plain_iteration_cycles():
+    """The oracle's iteration with the mu search (find_mu every iteration) on the small system: the
+    plain iteration settles into a two-cycle of mu, Newton-Krylov converges."""
+    s = system("small")
+    g = s.grid
+    integ, bz = O.HalfStoredIntegrals(s.V_half), O.NoSymBZ(s.mesh)
+    target = s.nel_from_G0()
+
+    def phi(G):
+        Gn = G.numpy()
+        dm = O.hf_density(Gn, s.ns)
+        F = O.hf_scalar(dm, s.S, 0.0, integ.pair, lambda X, k: X[k], s.nk, lambda ik: ik, s.NQ)
+        sig = O.gw_solve(Gn, integ, bz, g.Tnt_b, g.Ttn_b, s.ns, s.NQ)
+        ev = O.selfenergy_eigenspectra(F, sig, s.F, s.S, g.Tnt_f)
+        _, mu = O.find_mu(0.0, target, ev, g.Ttn_beta, g.wsample_f, s.ns, 1.0 / s.nk, 1e-12)
+        return torch.from_numpy(O.compute_G(F, sig, s.F, s.S, mu, g.Tnt_f, g.Ttn_f, g.wsample_f))
+
+    G0 = torch.from_numpy(s.G.copy())
+    _, hist = newton.newton_krylov(phi, G0, steps=10, atol=1e-10)
+    assert hist.residual[-1] < 1e-9
+    _, hp = newton.plain_iteration(phi, G0, 30)
+    assert min(hp.residual[-6:]) > 1.0

@@ -403,11 +403,9 @@ void invert_small_batched(const cplx* A, cplx* Ainv, int64_t nmat, int n, cudaSt
   require(n <= 64, GB200_ERR_INVALID, "invert_small_batched: n > 64");
   if (nmat <= 0) return;
   size_t smem = (size_t)(2 * n * n + n) * sizeof(cplx);
-  static bool attr_set = false;
-  if (!attr_set) {
-    GB_CUDA(cudaFuncSetAttribute(invert_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr_set = true;
-  }
+  // set on every call: the attribute belongs to the current device, and contexts on other devices
+  // or threads call this too (a host-side call of about a microsecond)
+  GB_CUDA(cudaFuncSetAttribute(invert_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   for (int64_t off = 0; off < nmat; off += 2147483647LL) {
     int64_t cnt = nmat - off < 2147483647LL ? nmat - off : 2147483647LL;
     invert_small_kernel<<<(unsigned)cnt, SMALL_NT, smem, st>>>(A + off * n * n, Ainv + off * n * n, n);
@@ -419,12 +417,8 @@ void invert_large_batched(const cplx* A, cplx* Ainv, cplx* aug, int64_t nmat, in
                           bool identity_minus, cudaStream_t st) {
   require(n <= 4096, GB200_ERR_INVALID, "invert_large_batched: n > 4096");
   if (nmat <= 0) return;
-  static bool attr_set = false;
-  if (!attr_set) {
-    GB_CUDA(cudaFuncSetAttribute(invert_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    GB_CUDA(cudaFuncSetAttribute(invert_blocked_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
-    attr_set = true;
-  }
+  GB_CUDA(cudaFuncSetAttribute(invert_large_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  GB_CUDA(cudaFuncSetAttribute(invert_blocked_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
   const size_t bsmem = blocked_smem_bytes(n);
   if (bsmem <= 220 * 1024) {
     // blocked elimination (panel in shared memory) for the sizes whose panel fits

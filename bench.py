@@ -374,7 +374,10 @@ def main_ours(args):
                                 "estimate": f"FP64 GW timed on q-points [0,{args.fp64_q}) x {s.nk}, rest of the iteration measured"}
             line["split_vs_fp64"] = fp64_iter / comp_s
             line["accuracy"] = {"max_abs_dSigma_sample": dsig, "max_abs_Sigma_sample": smax,
-                                "sample": f"partial Sigma of q-points [0,{args.fp64_q}), split vs FP64 GPU"}
+                                "sample": f"partial Sigma of q-points [0,{args.fp64_q}), split vs FP64 GPU",
+                                "max_abs_dSigma_full_estimate": dsig * s.nk / args.fp64_q,
+                                "full_estimate": "sample error x nq / q-points sampled (the q-point "
+                                                 "contributions' errors adding in phase)"}
         print(json.dumps(line), flush=True)
     if r["dist"]:
         r["dist"].barrier()

@@ -193,7 +193,7 @@ def blas_threads():
         return os.cpu_count()
 
 
-def setup_context(cfg, seed, slices, device, ws, rank):
+def setup_context(cfg, seed, slices, device, ws, rank, contraction_slices=None):
     from gb200 import lib, shard, solvers, synth
 
     s = synth.make_config(cfg, seed=seed, with_integrals=False)
@@ -205,6 +205,8 @@ def setup_context(cfg, seed, slices, device, ws, rank):
     synth.upload_device_integrals(ctx, s.nk, s.NQ, s.nao, seed=seed, device=device)
     ctx.set_hamiltonian(s.F, s.S)
     ctx.set_precision(lib.PREC_SPLIT, slices)
+    if contraction_slices:
+        ctx.set_contraction_slices(contraction_slices)
     if ws > 1:
         ctx.set_q_range(*shard.q_shard(s.nk, ws, rank))
     return s, ctx
@@ -222,7 +224,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(minutes=15))
     from gb200 import lib, shard
 
-    s, ctx = setup_context(args.config, args.seed, args.slices, local, ws, rank)
+    s, ctx = setup_context(args.config, args.seed, args.slices, local, ws, rank, args.contraction_slices)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
     sptr = stream.cuda_stream
@@ -348,7 +350,9 @@ def main_ours(args):
             "metric": METRIC, "value": 1.0 / comp_s, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": args.warmup,
             "ms_per_step": comp_s * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded generator; V generated on the GPU)",
-            "config": {"workload": WORKLOADS[args.config], "precision": f"split, {args.slices} INT8 slices",
+            "config": {"workload": WORKLOADS[args.config],
+                       "precision": f"split, {args.slices} INT8 slices" + (
+                           f" (per contraction a-f: {args.contraction_slices})" if args.contraction_slices else ""),
                        "parallelism": f"q-sharded over {ws} GPU(s), NCCL all-reduce of Sigma" if ws > 1 else "1 GPU",
                        "l2": "inputs larger than L2 (G 384 MB, V 100 GB): no flush"},
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": bf16_peak, "unit": "TFLOP/s",
@@ -398,7 +402,7 @@ def main_gw_profile(args):
     import torch
 
     torch.cuda.set_device(0)
-    s, ctx = setup_context(args.config, args.seed, args.slices, 0, 1, 0)
+    s, ctx = setup_context(args.config, args.seed, args.slices, 0, 1, 0, args.contraction_slices)
     G = torch.from_numpy(s.G).cuda()
     Sig = torch.empty_like(G)
     ctx.set_q_range(0, min(args.gw_q, s.nk))
@@ -503,6 +507,10 @@ def parse(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(WORKLOADS), default="c2")
     ap.add_argument("--slices", type=int, default=6)
+    ap.add_argument("--contraction-slices", dest="contraction_slices", default=None,
+                    type=lambda x: [int(v) for v in x.split(",")],
+                    help="slices of the six contractions P0 (a)-(c), Sigma (d)-(f), comma-separated; "
+                         "0 keeps --slices")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--fp64-q", dest="fp64_q", type=int, default=1, help="q-points timed for the FP64 comparison")
     ap.add_argument("--no-fp64-sample", action="store_true")

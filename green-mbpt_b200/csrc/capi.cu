@@ -248,6 +248,16 @@ int gb200_set_precision(gb200_context* ctx, int mode, int slices) {
   });
 }
 
+int gb200_set_contraction_slices(gb200_context* ctx, const int* slices6) {
+  return guarded(ctx, [&](Context& c) {
+    for (int i = 0; i < 6; ++i) {
+      const int s = slices6 ? slices6[i] : 0;
+      require(s == 0 || (s >= 2 && s <= 8), GB200_ERR_INVALID, "set_contraction_slices: slices must be 0 or in [2, 8]");
+      c.contraction_slices[i] = s;
+    }
+  });
+}
+
 int gb200_set_split_engine(gb200_context* ctx, int engine) {
   return guarded(ctx, [&](Context& c) {
     require(engine == 0 || engine == 1, GB200_ERR_INVALID, "set_split_engine: engine must be 0 or 1");

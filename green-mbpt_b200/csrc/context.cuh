@@ -76,6 +76,8 @@ struct Context {
   std::string last_error;
   int prec_mode = GB200_PREC_FP64;
   int slices = 4;
+  // slices of the P0 contractions (a)-(c) and the Sigma contractions (d)-(f); 0 takes `slices`
+  int contraction_slices[6] = {0, 0, 0, 0, 0, 0};
   int split_core = 0;             // 0: tcgen05 tensor cores, 1: CUDA-core validation core
   SplitEngine* split = nullptr;
 

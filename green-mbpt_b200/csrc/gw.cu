@@ -321,8 +321,8 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
   if (se) split_prepare_integrals(c, *se, st);
   // the P0 and Sigma contractions run in the selected precision; the
   // transforms and the aux-basis solve always run in FP64
-  auto contract = [&](const ZGemm& g) {
-    if (se) split_gemm(c, *se, g, st);
+  auto contract = [&](const ZGemm& g, int stage) {
+    if (se) split_gemm(c, *se, g, st, c.contraction_slices[stage]);
     else zgemm_fp64(g, st);
   };
 
@@ -377,9 +377,9 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
       cc.B.bat.s2 = (int64_t)kbk * ns * pe;
       cc.C.ptr = P0; cc.C.row = lin(1); cc.C.col = lin(NQ); cc.C.bat.s2 = (int64_t)NQ * NQ;
       cc.alpha = cmk(-pref, 0.0); cc.beta = cmk(1.0, 0.0);
-      contract(a);
-      contract(b);
-      contract(cc);
+      contract(a, 0);
+      contract(b, 1);
+      contract(cc, 2);
     }
     {
       int64_t total = (int64_t)nth * NQ * (NQ + 1) / 2;
@@ -468,9 +468,9 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
       f.C.ptr = Sigma + (int64_t)k0 * ge; f.C.row = lin(1); f.C.col = two(nao, nao, g_s);
       f.C.bat.s0 = ge;
       f.alpha = cmk(-1.0, 0.0); f.beta = cmk(1.0, 0.0);
-      contract(dd);
-      contract(e);
-      contract(f);
+      contract(dd, 3);
+      contract(e, 4);
+      contract(f, 5);
     }
     GB_CUDA(cudaEventRecord(c.ev[4], st));
     GB_CUDA(cudaEventSynchronize(c.ev[4]));

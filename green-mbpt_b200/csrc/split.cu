@@ -965,10 +965,10 @@ void run_slicer(SliceJob& j, int64_t nrb, cudaStream_t st) {
 
 }  // namespace
 
-void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st) {
+void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st, int slices) {
   if (g0.M <= 0 || g0.N <= 0) return;
   validate(g0);
-  const int S = c.slices;
+  const int S = slices > 0 ? slices : c.slices;
   require(S >= 2 && S <= 8, GB200_ERR_INVALID, "split: slices out of range");
   require(g0.K > 0, GB200_ERR_INVALID, "split: empty contraction");
   // One TMEM accumulator set of up to 512 columns and the widest tile it allows: the cost per

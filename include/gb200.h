@@ -114,6 +114,11 @@ int gb200_set_q0_correction(gb200_context* ctx, const double* AqQ, const double*
 /* Contraction precision (GB200_PREC_*) and, for GB200_PREC_SPLIT, the number
  * of INT8 slices per operand (2..8). */
 int gb200_set_precision(gb200_context* ctx, int mode, int slices);
+/* Slices per contraction under GB200_PREC_SPLIT: slices6[0..2] for the polarization contractions
+ * (P0_contraction, gw_cpu_kernel.cpp:200-215, in three GEMM stages) and slices6[3..5] for the
+ * self-energy ones (selfenergy_contraction, :359-373); 0 keeps the count of gb200_set_precision,
+ * NULL resets all six to 0.  No counterpart in the reference (which runs FP64). */
+int gb200_set_contraction_slices(gb200_context* ctx, const int* slices6);
 
 /* GW self-energy: Sigma(tau,k) from G(tau,k), both [nts, ns, nk, nso, nso].
  * Replaces gw_cpu_kernel::solve (gw_cpu_kernel.cpp:31-72): Sigma is zeroed,

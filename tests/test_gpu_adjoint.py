@@ -71,6 +71,23 @@ def test_gw_vjp_c4_finite_differences(gpu):
         assert abs(fd - an) <= 1e-6 * abs(fd)
 
 
+def test_gw_vjp_c4_matches_cpu_directional_derivatives(gpu):
+    """At the differentiable-step size, the adjoint against central differences (step 1e-6) of the
+    FP64 CPU oracle along fixed directions in G and V (tests/golden/make_c4_directional.py)."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "c4_directional.json")) as f:
+        d = json.load(f)
+    s = system(d["config"], d["generator_seed"])
+    Sb = _cotangent(s.G.shape, d["seed_cotangent"])
+    EG = _cotangent(s.G.shape, d["seed_dir_G"])
+    EV = _cotangent(s.V_half.shape, d["seed_dir_V"])
+    with solvers.make_context(s) as c:
+        Gb, Vb = c.gw_sigma_vjp(s.G, Sb, with_V=True)
+    assert abs(np.real(np.vdot(Gb, EG)) - d["fd_G"]) <= 1e-6 * abs(d["fd_G"])
+    assert abs(np.real(np.vdot(Vb, EV)) - d["fd_V"]) <= 1e-6 * abs(d["fd_V"])
+
+
 def test_gw_vjp_linearity(gpu):
     """Sigma[G] is not complex-analytic (P0 is hermitized), so its adjoint is linear in the
     cotangent over the reals: Gb(a Sb1 + Sb2) = a Gb(Sb1) + Gb(Sb2) for real a."""

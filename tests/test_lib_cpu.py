@@ -60,6 +60,8 @@ def test_create_rejects_bad_dims_without_gpu():
 def test_null_context_is_an_error():
     L = lib.load()
     assert L.gb200_gw_sigma(None, None, None) == lib.ERR_INVALID
+    assert L.gb200_set_contraction_slices(None, None) == lib.ERR_INVALID
+    assert L.gb200_gw_sigma_vjp(None, None, None, None, None) == lib.ERR_INVALID
     t = (ctypes.c_float * 4)()
     assert L.gb200_last_timings(None, t) == lib.ERR_INVALID
 

@@ -81,3 +81,21 @@ def test_newton_krylov_with_mu_search_where_plain_iteration_cycles():
     assert hist.residual[-1] < 1e-9
     _, hp = newton.plain_iteration(phi, G0, 30)
     assert min(hp.residual[-6:]) > 1.0
+
+
+def test_autograd_rejects_wrong_inputs_without_gpu():
+    """gb200.autograd.gw_sigma validates dtype, device and shape before any library call."""
+    from gb200 import autograd
+
+    class FakeDims:
+        nk, NQ, nao = 2, 3, 4
+
+    class FakeContext:
+        shape_G = (4, 1, 2, 4, 4)
+        dims = FakeDims()
+
+    c = FakeContext()
+    with pytest.raises(TypeError):
+        autograd.gw_sigma(c, torch.zeros(c.shape_G, dtype=torch.complex128))          # not on a GPU
+    with pytest.raises(TypeError):
+        autograd.gw_sigma(c, torch.zeros(c.shape_G, dtype=torch.complex64))

@@ -50,3 +50,4 @@ def test_oracle_vjp_V_matches_finite_differences(name):
         fd = (loss(s.V_half + h * E) - loss(s.V_half - h * E)) / (2 * h)
         an = np.real(np.sum(np.conj(Vb) * E))
         assert abs(fd - an) <= 1e-6 * abs(fd)
+

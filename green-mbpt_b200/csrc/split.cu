@@ -33,6 +33,7 @@
 #include <mutex>
 
 #include "split.cuh"
+#include "split_digits.cuh"
 
 namespace gb200 {
 
@@ -268,7 +269,7 @@ __device__ __forceinline__ void load_slice_tile(const SliceJob& j, const cplx* b
   }
 }
 
-// Pass 1: per-row exponent e (max |Re|,|Im| < 2^e) by atomicMax over K tiles.
+// Pass 1: per-row exponent e' = e + 1 (max |Re|,|Im| < 2^e = 2^(e'-1)) by atomicMax over K tiles.
 __global__ void __launch_bounds__(SL_NT, 4) slice_expo_kernel(SliceJob j) {
   __shared__ cplx tile[TR][TKP];
   __shared__ int64_t roff[TR], koff[TK];
@@ -293,33 +294,12 @@ __global__ void __launch_bounds__(SL_NT, 4) slice_expo_kernel(SliceJob j) {
   if (part == 0 && m > 0.0 && r0 + rl < j.R) {
     int e;
     frexp(m, &e);
-    atomicMax(&j.expo[rb * j.e_ld + r0 + rl], e);
+    atomicMax(&j.expo[rb * j.e_ld + r0 + rl], e + 1);  // |a| < 2^(e'-1): one bit of headroom
   }
 }
 
-// Ozaki digits of one real number: with X = trunc(a * 2^(7S - e)) (exact conversion, |X| < 2^(7S)),
-// slice s is the s-th base-128 digit of |X| from the top, carrying the sign of a.  This equals
-// the truncation cascade q_s = trunc(x_s), x_{s+1} = 128 (x_s - q_s) with x_0 = a 2^(7-e).
-struct Digits {
-  uint64_t mag;
-  uint32_t neg;  // 0 or 0xFFFFFFFF
-};
-
-__device__ __forceinline__ Digits digits_of(double a, double scale) {
-  const long long X = __double2ll_rz(a * scale);
-  Digits d;
-  d.neg = X < 0 ? 0xFFFFFFFFu : 0u;
-  d.mag = (uint64_t)(X < 0 ? -X : X);
-  return d;
-}
-
-// signed digit (top = 0) of magnitude `mag` as a byte in the low 8 bits; bit 0 of `neg` is the sign
-__device__ __forceinline__ uint32_t digit_byte(uint64_t mag, uint32_t neg, int shift) {
-  const uint32_t m = 0u - (neg & 1u);  // 0 or 0xFFFFFFFF
-  uint32_t q = (uint32_t)(mag >> shift) & 127u;
-  q = (q ^ m) - m;  // conditional negate
-  return q & 0xFFu;
-}
+// Ozaki digits of one real number: balanced base-128 digits of X = rint(a 2^(7S - e)), with one bit
+// of headroom in the row exponent e (split_digits.cuh).
 
 // Write the S digit planes of 8 consecutive K positions (from k) of row r with row exponent e,
 // including the zero padding of rows and K.
@@ -333,29 +313,25 @@ __device__ __forceinline__ void write_digits(const SliceJob& j, const cplx (&val
   const int ex1 = max(-1000, min(1000, ex));
   const double sc1 = __longlong_as_double((long long)(ex1 + 1023) << 52);
   const double sc2 = __longlong_as_double((long long)(max(-1022, min(1023, ex - ex1)) + 1023) << 52);
-  // magnitudes of the truncated scaled values and their signs (one bit per real part)
-  uint64_t mr[8], mi[8];
-  uint32_t negs = 0;
+  // X + bias of the rounded scaled values (two's complement wrap-around gives X + bias >= 0)
+  const uint64_t bias = balanced_bias(S);
+  uint64_t ur[8], ui[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const cplx v = vals[i];
-    const Digits a = digits_of(v.x * sc1, sc2), b = digits_of(v.y * sc1, sc2);
-    mr[i] = a.mag;
-    mi[i] = b.mag;
-    negs |= (a.neg & 1u) << (2 * i);
-    negs |= (b.neg & 1u) << (2 * i + 1);
+    ur[i] = (uint64_t)__double2ll_rn((v.x * sc1) * sc2) + bias;
+    ui[i] = (uint64_t)__double2ll_rn((v.y * sc1) * sc2) + bias;
   }
   const int64_t plane = j.rows_pad * j.kpad;
   int8_t* outb = j.out + rb * (int64_t)S * plane;
   for (int s = 0; s < S; ++s) {
-    const int shift = 7 * (S - 1 - s);
     uint32_t w0[4], w1[4];
 #pragma unroll
     for (int h = 0; h < 4; ++h) {
-      const uint32_t r0b = digit_byte(mr[2 * h], negs >> (4 * h), shift);
-      const uint32_t i0b = digit_byte(mi[2 * h], negs >> (4 * h + 1), shift);
-      const uint32_t r1b = digit_byte(mr[2 * h + 1], negs >> (4 * h + 2), shift);
-      const uint32_t i1b = digit_byte(mi[2 * h + 1], negs >> (4 * h + 3), shift);
+      const uint32_t r0b = balanced_digit_byte(ur[2 * h], S, s);
+      const uint32_t i0b = balanced_digit_byte(ui[2 * h], S, s);
+      const uint32_t r1b = balanced_digit_byte(ur[2 * h + 1], S, s);
+      const uint32_t i1b = balanced_digit_byte(ui[2 * h + 1], S, s);
       if (j.embed) {
         // row 2r: (re, -im) pairs; row 2r+1: (im, re) pairs
         const uint32_t ni0 = (0u - i0b) & 0xFFu, ni1 = (0u - i1b) & 0xFFu;
@@ -400,7 +376,10 @@ __global__ void __launch_bounds__(SL_NT, 4) slice_write_kernel(SliceJob j) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) m = fmax(m, fmax(fabs(vals[i].x), fabs(vals[i].y)));
     for (int o = 4; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (m > 0.0) frexp(m, &e);
+    if (m > 0.0) {
+      frexp(m, &e);
+      ++e;  // one bit of headroom, as in slice_expo_kernel
+    }
     if (grp == 0 && r < j.R) j.expo[rb * j.e_ld + r] = e;
   } else if (r < j.R) {
     e = j.expo[rb * j.e_ld + r];
@@ -440,7 +419,10 @@ __global__ void __launch_bounds__(SL_NT, 3) slice_fused_kernel(SliceJob j, int n
   }
   const int64_t r = r0 + rl;
   int e = 0;
-  if (rmax[rl] > 0.0) frexp(rmax[rl], &e);
+  if (rmax[rl] > 0.0) {
+    frexp(rmax[rl], &e);
+    ++e;  // one bit of headroom, as in slice_expo_kernel
+  }
   if (grp == 0 && r < j.R) j.expo[rb * j.e_ld + r] = e;
   for (int kt = 0; kt < nkt; ++kt) {
     const int64_t kc = (int64_t)kt * TK;

@@ -39,3 +39,27 @@ def test_split_error_vs_fp64(gpu, name):
         errs[S] = float(np.abs(sigma_split(s, S, 0) - ref).max())
     assert errs[4] < errs[3] and errs[5] < errs[4]
     assert errs[5] <= 1e-8, errs
+
+
+def test_full_sigma_within_bound_on_workload_shapes(gpu):
+    """One whole iteration from G0, split (5 slices) against FP64, on a system with the headline
+    workload's shapes (nao=40, naux=250, ntau=120, nw=120, beta=200, eps ~ U[-5,5]) and a 2x1x1
+    mesh: the full self-energy within 1e-8 Ha (|Sigma| reaches about 32 Ha here), G within 1e-9."""
+    import torch
+    from gb200 import synth
+    s = synth.make_system(mesh=(2, 1, 1), nao=40, naux=250, ns=1, beta=200.0, nts=120, nw=120, eps_range=5.0,
+                          seed=0)
+    out = {}
+    for name, prec in (("fp64", lib.PREC_FP64), ("split", lib.PREC_SPLIT)):
+        with solvers.make_context(s, precision=prec, slices=5) as c:
+            G = torch.tensor(s.G, dtype=torch.complex128, device="cuda")
+            d = c.dims
+            S1 = torch.empty((d.ns, d.nk, d.nso, d.nso), dtype=torch.complex128, device="cuda")
+            Sig = torch.empty_like(G)
+            torch.cuda.synchronize()
+            c.iteration_device(G.data_ptr(), S1.data_ptr(), Sig.data_ptr(), 0.0, s.nel_from_G0(), 1e-9, 0.0,
+                               stream=0x1, energies=True)
+            torch.cuda.synchronize()
+            out[name] = (G.cpu().numpy(), Sig.cpu().numpy())
+    assert np.abs(out["split"][1] - out["fp64"][1]).max() <= 1e-8
+    assert np.abs(out["split"][0] - out["fp64"][0]).max() <= 1e-9

@@ -17,3 +17,17 @@ def test_split_model_error_falls_by_the_digit_base():
     Ai = rng.integers(-50, 50, (8, 12)) + 1j * rng.integers(-50, 50, (8, 12))
     Bi = rng.integers(-50, 50, (12, 6)) + 1j * rng.integers(-50, 50, (12, 6))
     assert np.array_equal(SM.split_mm(Ai, Bi, 3), Ai @ Bi)
+
+
+def test_balanced_digits_remove_the_bias_of_truncation():
+    """For sums of same-signed products (the sign-correlated case), truncation toward zero biases
+    every term the same way and its error grows with the contraction length; rounding to nearest
+    with balanced digits does not."""
+    import split_model as SM
+    rng = np.random.default_rng(4)
+    A = rng.uniform(0.5, 1.0, (16, 4000)) + 0j
+    B = rng.uniform(0.5, 1.0, (4000, 8)) + 0j
+    ref = A @ B
+    trunc = np.abs(SM.split_mm(A, B, 4, "truncated") - ref).max()
+    bal = np.abs(SM.split_mm(A, B, 4) - ref).max()
+    assert bal < trunc / 10

@@ -4,13 +4,15 @@
 //
 // Number format.  Every complex row of the left operand (and every complex
 // column of the right one) gets a power-of-two exponent e with max|Re|,|Im| <
-// 2^e over the contraction range.  Each real part is cut into S signed 7-bit
-// slices by truncation, a = 2^(e-7) (q_0 + q_1 2^-7 + ... + q_{S-1} 2^-7(S-1)) + r,
-// |q_s| <= 127, which is exact in FP64 at every step.  Products of slices s and
-// t share the weight 2^-7(s+t); all pairs with s + t = d accumulate into one
-// INT32 accumulator "diagonal" d (pairs with s + t >= S are dropped, the usual
-// triangular Ozaki truncation).  The host splits the contraction so that no
-// diagonal can overflow INT32.
+// 2^(e-1) over the contraction range (one bit of headroom).  Each real part is
+// rounded to X = rint(a 2^(7S-e)) and cut into S balanced base-128 digits,
+// a = 2^(e-7) (q_0 + q_1 2^-7 + ... + q_{S-1} 2^-7(S-1)) + r with q_s in [-64, 64]
+// (split_digits.cuh).  Products of slices s and t share the weight 2^-7(s+t); all
+// pairs with s + t = d accumulate into one INT32 accumulator "diagonal" d (pairs
+// with s + t >= S are dropped, the usual triangular Ozaki truncation).  Rounding
+// and balanced digits keep the representation error and the dropped products
+// zero-mean, so they do not add up in phase along the contraction.  The host
+// splits the contraction so that no diagonal can overflow INT32.
 //
 // Complex arithmetic.  A complex product becomes one real product through the
 // embedding  [Re A  -Im A; Im A  Re A] x [Re B; Im B]: the left operand is stored

@@ -1,16 +1,19 @@
 """Minimal read-only HDF5 reader (pure Python + numpy + zlib).
 
-It covers what green-mbpt's input and integral files use: superblock v0/v1,
-version-1 object headers with continuation blocks, old-style groups
-(symbol-table message -> v1 group B-tree -> SNOD nodes + local heap),
-contiguous / compact / chunked (v1 chunk B-tree) layouts, the deflate and
-shuffle filters, fixed-point, floating-point and string datatypes, and
-attributes.  There is no h5py or libhdf5 in this environment; gb200.inputs
+It covers what green-mbpt's input, integral and result files use:
+- superblocks v0/v1 and v2/v3;
+- version-1 object headers, and version-2 ones ("OHDR" with "OCHK" continuation chunks);
+- old-style groups (symbol-table message -> v1 group B-tree -> SNOD nodes + local heap), and new-style groups with their links stored compactly in the object header;
+- contiguous and compact layouts;
+- chunked layouts indexed by a v1 B-tree, by a single chunk or implicitly;
+- the deflate and shuffle filters;
+- fixed-point, floating-point, string, compound and variable-length datatypes, and attributes.  There is no h5py or libhdf5 in this environment; gb200.inputs
 reads the solver's input files with it.
 
 The format facts used here follow the public HDF5 File Format Specification
 (version 3.0), sections II (superblock), III.A/B (B-trees, symbol table
-nodes), III.D (local heap), IV.A (object headers) and IV.A.2 (messages).
+nodes), III.D (local heap), IV.A (object headers) and IV.A.2 (messages:
+link info, link and data layout among them).
 """
 from __future__ import annotations
 
@@ -42,6 +45,15 @@ class H5File:
         if b[:8] != _SIG:
             raise H5Error(f"{path}: not an HDF5 file")
         ver = b[8]
+        self._cache = {}
+        if ver in (2, 3):
+            # signature, version, offset/length sizes, flags, base, extension, eof, root header, checksum
+            self.so, self.sl = b[9], b[10]
+            if self.so != 8 or self.sl != 8:
+                raise H5Error("only 8-byte offsets/lengths supported")
+            self.base = self._u(12, 8)
+            self.root_addr = self._u(36, 8)
+            return
         if ver not in (0, 1):
             raise H5Error(f"{path}: superblock version {ver} not supported")
         self.so = b[13]
@@ -53,7 +65,6 @@ class H5File:
         p += 4 * 8  # base, free-space, eof, driver
         # root symbol table entry
         self.root_addr = self._u(p + 8, 8)
-        self._cache = {}
 
     # -- primitive readers -------------------------------------------------
     def _u(self, off, n):
@@ -65,7 +76,9 @@ class H5File:
             return self._cache[addr]
         b = self.buf
         if b[addr:addr + 4] == b"OHDR":
-            raise H5Error("version-2 object headers are not supported")
+            msgs = self._messages_v2(addr)
+            self._cache[addr] = msgs
+            return msgs
         if b[addr] != 1:
             raise H5Error(f"object header version {b[addr]} at {addr:#x}")
         nmsg = self._u(addr + 2, 2)
@@ -85,6 +98,42 @@ class H5File:
                     blocks.append((int.from_bytes(data[0:8], "little"), int.from_bytes(data[8:16], "little")))
                 msgs.append((mtype, data))
         self._cache[addr] = msgs
+        return msgs
+
+    def _messages_v2(self, addr):
+        """Messages of a version-2 object header: chunk 0 after the prefix, more chunks ("OCHK")
+        named by continuation messages; each chunk ends with a 4-byte checksum."""
+        b = self.buf
+        if b[addr + 4] != 2:
+            raise H5Error(f"object header version {b[addr + 4]} at {addr:#x}")
+        flags = b[addr + 5]
+        p = addr + 6
+        if flags & 0x20:
+            p += 16  # access, modification, change, birth times
+        if flags & 0x10:
+            p += 4  # attribute phase-change values
+        nb = 1 << (flags & 3)
+        size0 = self._u(p, nb)
+        p += nb
+        order = 2 if flags & 0x04 else 0  # creation order field in every message header
+        blocks = [(p, p + size0)]
+        msgs = []
+        while blocks:
+            start, end = blocks.pop(0)
+            q = start
+            while q + 4 + order <= end:
+                mtype = b[q]
+                msize = self._u(q + 1, 2)
+                q += 4 + order
+                data = b[q:q + msize]
+                q += msize
+                if mtype == 0x10:  # continuation: address and length of an OCHK block
+                    ca = int.from_bytes(data[0:8], "little")
+                    cl = int.from_bytes(data[8:16], "little")
+                    if b[ca:ca + 4] != b"OCHK":
+                        raise H5Error("bad object header continuation signature")
+                    blocks.append((ca + 4, ca + cl - 4))
+                msgs.append((mtype, data))
         return msgs
 
     # -- groups ------------------------------------------------------------
@@ -132,13 +181,49 @@ class H5File:
                         q += 40
         return out
 
+    @staticmethod
+    def _link(data):
+        """(name, object header address) of a hard link message; None for soft/external links."""
+        flags = data[1]
+        p = 2
+        ltype = 0
+        if flags & 0x08:
+            ltype = data[p]
+            p += 1
+        if flags & 0x04:
+            p += 8  # creation order
+        if flags & 0x10:
+            p += 1  # name character set
+        nb = 1 << (flags & 3)
+        n = int.from_bytes(data[p:p + nb], "little")
+        p += nb
+        name = data[p:p + n].decode()
+        p += n
+        if ltype != 0:
+            return None
+        return name, int.from_bytes(data[p:p + 8], "little")
+
     def _children(self, addr):
-        for mtype, data in self._messages(addr):
+        msgs = self._messages(addr)
+        for mtype, data in msgs:
             if mtype == 0x11:
                 bt = int.from_bytes(data[0:8], "little")
                 hp = int.from_bytes(data[8:16], "little")
                 return self._group_entries(bt, hp)
-        return None
+        if not any(m in (0x02, 0x06, 0x0A) for m, _ in msgs):
+            return None
+        for mtype, data in msgs:
+            if mtype == 0x02:  # link info: links in a fractal heap when its address is defined
+                p = 2 + (8 if data[1] & 0x01 else 0)
+                if int.from_bytes(data[p:p + 8], "little") != UNDEF:
+                    raise H5Error("groups with densely stored links are not supported")
+        out = {}
+        for mtype, data in msgs:
+            if mtype == 0x06:
+                ln = self._link(data)
+                if ln is not None:
+                    out[ln[0]] = ln[1]
+        return out
 
     def _resolve(self, path):
         addr = self.root_addr
@@ -347,7 +432,9 @@ class H5File:
         ver = lay[0]
         nelem = int(np.prod(shape)) if shape else 1
         total = nelem * itemsize
-        if ver == 3:
+        if ver == 4 and lay[1] == 2:
+            return self._chunked_v4(lay, shape, itemsize, filters)
+        if ver in (3, 4):
             cls = lay[1]
             if cls == 0:
                 size = int.from_bytes(lay[2:4], "little")
@@ -378,6 +465,45 @@ class H5File:
                 return self.buf[addr:addr + total]
             return self._chunked(addr, shape, dims[:-1], itemsize, filters)
         raise H5Error(f"layout version {ver} not supported")
+
+    def _chunked_v4(self, lay, shape, itemsize, filters):
+        """Version-4 chunked layout with a single-chunk (1) or implicit (2) index."""
+        flags, nd, enc = lay[2], lay[3], lay[4]
+        p = 5
+        dims = [int.from_bytes(lay[p + enc * i:p + enc * (i + 1)], "little") for i in range(nd)]
+        p += enc * nd
+        cdims = dims[:-1]  # the last one is the element size
+        itype = lay[p]
+        p += 1
+        nelem = int(np.prod(shape)) if shape else 1
+        if itype == 1:
+            csize = mask = None
+            if flags & 0x02:  # filtered single chunk: its size and filter mask precede the address
+                csize = int.from_bytes(lay[p:p + 8], "little")
+                mask = int.from_bytes(lay[p + 8:p + 12], "little")
+                p += 12
+            addr = int.from_bytes(lay[p:p + 8], "little")
+            if addr == UNDEF:
+                return bytes(nelem * itemsize)
+            if csize is None:
+                return self.buf[addr:addr + nelem * itemsize]
+            raw = self._unfilter(self.buf[addr:addr + csize], filters, mask, itemsize)
+            return raw[:nelem * itemsize]
+        if itype == 2:
+            addr = int.from_bytes(lay[p:p + 8], "little")
+            nd_ = len(shape)
+            grid = [-(-s // c) for s, c in zip(shape, cdims)]
+            csz = int(np.prod(cdims)) * itemsize
+            out = np.zeros(tuple(shape) + (itemsize,), dtype=np.uint8)
+            for i, idx in enumerate(np.ndindex(*grid)):
+                c = np.frombuffer(self.buf[addr + i * csz:addr + (i + 1) * csz], dtype=np.uint8)
+                c = c.reshape(tuple(cdims) + (itemsize,))
+                sl_out = tuple(slice(k * d, min(k * d + d, s)) for k, d, s in zip(idx, cdims, shape))
+                sl_in = tuple(slice(0, so.stop - so.start) for so in sl_out)
+                out[sl_out] = c[sl_in]
+            del nd_
+            return out.tobytes()
+        raise H5Error(f"chunk index type {itype} not supported")
 
     def _chunked(self, bt, shape, cdims, itemsize, filters):
         nd = len(shape)

@@ -178,6 +178,31 @@ def test_hf_x2c_golden_through_gpu(gpu):
     assert np.abs(F - np.conj(np.swapaxes(F, -1, -2))).max() < 1e-11 * np.abs(F).max()
 
 
+def test_hf_orth_invariance_golden_through_gpu(gpu):
+    """HF part of the reference's orth-invariance test (test/solvers_test.cpp:296-430) through the
+    GPU Fock build: one H2 molecule in four orbital bases; F equals the reference run's Sigma1,
+    E_1b and E_HF + E_nuc the energies it wrote (dyson.cpp:325-326), and the energies agree across
+    the bases, all to 1e-10."""
+    d = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "hf_orth.npz")))
+    E = {}
+    for basis in ("none", "lowdin", "mo", "natural"):
+        ns, nk, nao, nso, NQ = (int(x) for x in d[f"{basis}/dims"])
+        dm = -1.0 * d[f"{basis}/G_beta"]  # ns = 2: spin prefactor -1 (hf_solver.h:38)
+        H = d[f"{basis}/H"]
+        with lib.Context(nk, nao, ns, NQ, 2, 2, 2, 100.0) as c:
+            c.set_integrals(np.ascontiguousarray(d[f"{basis}/V_chunk"].reshape(1, NQ, nao, nao)), lib.INTEGRALS_HF)
+            F = c.hf_fock(dm, d[f"{basis}/S"], float(d[f"{basis}/madelung"]))
+        np.testing.assert_allclose(F, d[f"{basis}/Sigma1"], rtol=0, atol=1e-10)
+        e1 = sum(np.trace(dm[s, 0] @ H[s, 0]).real for s in range(ns))
+        ehf = sum(0.5 * np.trace(dm[s, 0] @ (F[s, 0] + 2.0 * H[s, 0])).real for s in range(ns))
+        assert abs(e1 - float(d[f"{basis}/Energy_1b"])) < 1e-10
+        assert abs(ehf + float(d[f"{basis}/E_nuc"]) - float(d[f"{basis}/Energy_HF"])) < 1e-10
+        E[basis] = (e1, ehf)
+    for basis in ("lowdin", "mo", "natural"):
+        assert abs(E[basis][0] - E["none"][0]) < 1e-10
+        assert abs(E[basis][1] - E["none"][1]) < 1e-10
+
+
 def test_hf_x2c_matches_oracle_with_madelung(gpu):
     """X2C Fock build with a non-zero Madelung constant and several k-points against the oracle."""
     s = system("small")

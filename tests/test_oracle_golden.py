@@ -54,3 +54,36 @@ def test_oracle_detects_planted_error():
     F = O.hf_scalar(dm, d["S_ibz"], float(d["madelung"]), lambda a, b: sym.integral(d["V_chunk"], a, b),
                     sym.value_AO, nk, sym.full_point, NQ)
     assert np.abs(F - d["Sigma1"]).max() > 1e-10
+
+
+ORTH_BASES = ("none", "lowdin", "mo", "natural")
+
+
+def orth_case(d, basis):
+    ns, nk, nao, nso, NQ = (int(x) for x in d[f"{basis}/dims"])
+    V = d[f"{basis}/V_chunk"].reshape(-1, NQ, nso, nso)
+    return ns, nk, NQ, V
+
+
+def test_hf_orth_invariance_golden():
+    """HF part of the reference's orth-invariance test (test/solvers_test.cpp:296-430) on one H2
+    molecule written in four orbital bases: from each basis's G(beta), the oracle's Fock matrix
+    equals the reference run's iter1/Sigma1, E_1b and E_HF + E_nuc equal the energies it wrote
+    (dyson.cpp:325-326), and both energies agree across the bases, all to 1e-10."""
+    d = dict(np.load(os.path.join(HERE, "hf_orth.npz")))
+    E = {}
+    for basis in ORTH_BASES:
+        ns, nk, NQ, V = orth_case(d, basis)
+        dm = O.hf_density(d[f"{basis}/G_beta"][None], ns)
+        F = O.hf_scalar(dm, d[f"{basis}/S"], float(d[f"{basis}/madelung"]), lambda a, b: V[0], lambda X, k: X[k],
+                        nk, lambda ik: ik, NQ)
+        np.testing.assert_allclose(F, d[f"{basis}/Sigma1"], rtol=0, atol=1e-10)
+        G = d[f"{basis}/G_beta"][None]
+        e1, ehf, ec = O.compute_energy(G, F, np.zeros_like(G), d[f"{basis}/H"], np.ones((1, 1)), np.ones(1), 1.0 / nk)
+        assert ec == 0.0
+        assert abs(e1 - float(d[f"{basis}/Energy_1b"])) < 1e-10
+        assert abs(ehf + float(d[f"{basis}/E_nuc"]) - float(d[f"{basis}/Energy_HF"])) < 1e-10
+        E[basis] = (e1, ehf)
+    for basis in ORTH_BASES[1:]:
+        assert abs(E[basis][0] - E["none"][0]) < 1e-10
+        assert abs(E[basis][1] - E["none"][1]) < 1e-10

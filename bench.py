@@ -226,7 +226,10 @@ def run_ours(args):
     s, ctx = setup_context(args.config, args.seed, args.slices, local, ws, rank, args.contraction_slices)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
-    sptr = stream.cuda_stream
+    # the library runs on torch's stream, so its work is ordered with the copies around it; a null
+    # handle would select the context's own non-blocking stream, so the default stream is passed
+    # by its legacy handle
+    sptr = stream.cuda_stream or 0x1
     G0 = torch.from_numpy(s.G).pin_memory()
     Gout = torch.empty_like(G0).pin_memory()
     G = torch.empty(s.G.shape, dtype=torch.complex128, device=dev)

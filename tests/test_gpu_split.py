@@ -44,7 +44,9 @@ def test_split_error_vs_fp64(gpu, name):
 def test_full_sigma_within_bound_on_workload_shapes(gpu):
     """One whole iteration from G0, split (5 slices) against FP64, on a system with the headline
     workload's shapes (nao=40, naux=250, ntau=120, nw=120, beta=200, eps ~ U[-5,5]) and a 2x1x1
-    mesh: the full self-energy within 1e-8 Ha (|Sigma| reaches about 32 Ha here), G within 1e-9."""
+    mesh: the full self-energy within 1e-8 Ha (|Sigma| reaches about 32 Ha here).  G also goes
+    through the chemical-potential bisection (tolerance 1e-9), which can stop one interval apart in
+    the two runs, so it is held to 1e-8."""
     import torch
     from gb200 import synth
     s = synth.make_system(mesh=(2, 1, 1), nao=40, naux=250, ns=1, beta=200.0, nts=120, nw=120, eps_range=5.0,
@@ -62,4 +64,4 @@ def test_full_sigma_within_bound_on_workload_shapes(gpu):
             torch.cuda.synchronize()
             out[name] = (G.cpu().numpy(), Sig.cpu().numpy())
     assert np.abs(out["split"][1] - out["fp64"][1]).max() <= 1e-8
-    assert np.abs(out["split"][0] - out["fp64"][0]).max() <= 1e-9
+    assert np.abs(out["split"][0] - out["fp64"][0]).max() <= 1e-8

@@ -17,7 +17,8 @@ link info, link and data layout among them).
 """
 from __future__ import annotations
 
-import struct
+import mmap
+import os
 import zlib
 
 import numpy as np
@@ -38,8 +39,11 @@ class _Dtype:
 
 class H5File:
     def __init__(self, path: str):
+        # mapped, not read: integral files run to gigabytes and only the touched pages are loaded
         with open(path, "rb") as fh:
-            self.buf = fh.read()
+            if os.fstat(fh.fileno()).st_size == 0:
+                raise H5Error(f"{path}: empty file")
+            self.buf = mmap.mmap(fh.fileno(), 0, access=mmap.ACCESS_READ)
         self.path = path
         b = self.buf
         if b[:8] != _SIG:
@@ -146,7 +150,9 @@ class H5File:
     def _heap_str(self, heap_data, off):
         b = self.buf
         s = heap_data + off
-        e = b.index(b"\x00", s)
+        e = b.find(b"\x00", s)
+        if e < 0:
+            raise H5Error("unterminated local heap string")
         return b[s:e].decode()
 
     def _group_entries(self, btree, heap):

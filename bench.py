@@ -396,7 +396,12 @@ def main_ours(args):
                          "traffic_unit": "bytes per launch (scaled from the c2k2 ncu capture at 5 slices, "
                                          "by the launch's flops and by slices / 5 for the digit planes)",
                          "kernel": "split_gemm_tc_kernel (tcgen05 kind::i8)", "launches": r["tc_n"],
-                         "peak_source": f"{peak_src} bf16 dense sustained; achieved counts FP64-equivalent complex flops"},
+                         "peak_source": f"{peak_src} bf16 dense sustained; achieved counts FP64-equivalent complex flops",
+                         # the INT8 work behind those flops: S(S+1)/2 digit-plane products, each 4MKN
+                         # multiply-adds over the real embedding, per complex product (8MKN flops)
+                         "int8_tops": (achieved * args.slices * (args.slices + 1) / 2) if achieved else None,
+                         "int8_frac_of_2x_bf16": (achieved * args.slices * (args.slices + 1) / 2 / (2 * bf16_peak))
+                         if achieved else None},
             "cpu_baseline": {"value": 1.0 / cpu_est, "unit": UNIT, "cores": blas_threads(), "kind": "port",
                              "sample": cpu_desc},
             "e2e": {"value": 1.0 / tot_s, "unit": UNIT, "h2d_bytes_per_step": r["bytes_io"],

@@ -502,6 +502,7 @@ def main_newton(args):
     out = {"workload": WORKLOADS[args.config], "precision": "FP64", "gw_sigma_ms": t_fwd,
            "vjp_G_ms": t_vjp, "vjp_G_V_ms": t_vjp_v}
     for name, run in (("plain", lambda: newton.plain_iteration(it, G, args.newton)),
+                      ("plain_g_mixing_0.5", lambda: newton.plain_iteration(it, G, args.newton, mixing=0.5)),
                       ("newton_krylov", lambda: newton.newton_krylov(it, G, args.newton, maxiter=30,
                                                                       atol=atol))):
         torch.cuda.synchronize()

@@ -91,8 +91,9 @@ class History:
     krylov: list = field(default_factory=list)
 
 
-def plain_iteration(phi, G0: torch.Tensor, steps: int):
-    """G <- Phi(G), `steps` times; the residual of step i is |Phi(G_i) - G_i|."""
+def plain_iteration(phi, G0: torch.Tensor, steps: int, mixing: float = 1.0):
+    """G <- (1 - w) G + w Phi(G), `steps` times (w = `mixing`; 1 is the bare iteration, w < 1 the
+    damped G mixing of green-sc's G_MIXING with weight w); the residual of step i is |Phi(G_i) - G_i|."""
     G = G0.clone()
     hist = History()
     evals = 0
@@ -101,7 +102,7 @@ def plain_iteration(phi, G0: torch.Tensor, steps: int):
         evals += 1
         hist.residual.append(_norm(G1 - G))
         hist.evaluations.append(evals)
-        G = G1
+        G = G1 if mixing == 1.0 else (1.0 - mixing) * G + mixing * G1
     return G, hist
 
 

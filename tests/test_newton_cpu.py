@@ -81,6 +81,10 @@ def test_newton_krylov_with_mu_search_where_plain_iteration_cycles():
     assert hist.residual[-1] < 1e-9
     _, hp = newton.plain_iteration(phi, G0, 30)
     assert min(hp.residual[-6:]) > 1.0
+    # damped G mixing (weight 0.5) breaks the cycle and converges linearly, more slowly than Newton
+    _, hm = newton.plain_iteration(phi, G0, 30, mixing=0.5)
+    assert hm.residual[-1] < 1e-5
+    assert hm.residual[-1] > 100 * hist.residual[-1]
 
 
 def test_autograd_rejects_wrong_inputs_without_gpu():

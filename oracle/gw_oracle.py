@@ -1,8 +1,8 @@
 """FP64 CPU oracle for the density-fitted GW / HF / Dyson path of green-mbpt.
 
-TEST INFRASTRUCTURE ONLY.  This module is the checker that the CUDA library
-is compared against; only tests, the smoke check and the CPU-baseline leg of
-the benchmark may import it.  The library never calls it.
+TEST INFRASTRUCTURE ONLY.  The CUDA library's results are compared against this
+module; only tests, the smoke check and the CPU-baseline leg of the benchmark
+may import it.  The library never calls it.
 
 It restates, in numpy (complex128, BLAS zgemm through ``@``), the reference's
 algorithm with the same contraction order, prefactors, signs and loop

@@ -248,6 +248,13 @@ int gb200_set_precision(gb200_context* ctx, int mode, int slices) {
   });
 }
 
+int gb200_set_memory_budget(gb200_context* ctx, double bytes) {
+  return guarded(ctx, [&](Context& c) {
+    require(bytes >= 0.0, GB200_ERR_INVALID, "set_memory_budget: negative budget");
+    c.mem_budget = bytes;
+  });
+}
+
 int gb200_set_contraction_slices(gb200_context* ctx, const int* slices6) {
   return guarded(ctx, [&](Context& c) {
     for (int i = 0; i < 6; ++i) {

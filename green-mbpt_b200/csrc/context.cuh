@@ -78,6 +78,15 @@ struct Context {
   int slices = 4;
   // slices of the P0 contractions (a)-(c) and the Sigma contractions (d)-(f); 0 takes `slices`
   int contraction_slices[6] = {0, 0, 0, 0, 0, 0};
+  // bytes the blocked intermediates of one call may take (GW: the two k-block buffers; HF: the
+  // exchange intermediates); 0 takes a default share of the free device memory
+  double mem_budget = 0.0;
+  double budget_or(double cap, double free_share) const {
+    if (mem_budget > 0.0) return mem_budget;
+    size_t free_b = 0, total_b = 0;
+    GB_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    return std::min(cap, free_share * (double)free_b);
+  }
   int split_core = 0;             // 0: tcgen05 tensor cores, 1: CUDA-core validation core
   SplitEngine* split = nullptr;
 

@@ -159,10 +159,8 @@ void build_hf_tables(Context& c) {
 
 // Choose the k-block size so that the two largest intermediates fit the budget.
 static int choose_kblock(const Context& c, int64_t elems_per_k) {
-  size_t free_b = 0, total_b = 0;
-  GB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  // leave headroom; at most 24 GB for the GW intermediates
-  double budget = std::min<double>(24e9, 0.6 * (double)free_b);
+  // leave headroom; at most 24 GB for the GW intermediates unless the caller set a budget
+  const double budget = c.budget_or(24e9, 0.6);
   double per_k = 2.0 * (double)elems_per_k * sizeof(cplx);
   int kb = (int)std::max(1.0, std::floor(budget / per_k));
   return std::min(kb, c.d.nk);

@@ -141,9 +141,7 @@ void gw_sigma_vjp(Context& c, const cplx* G, const cplx* Sb, cplx* Gb, cplx* Vb,
   cplx* P0hb = buf(SL_ADJ_P0HB, nth * nq2);
   // k-block: three intermediates of nts*ns*pe per k-point
   const int64_t blk = (int64_t)nts * ns * pe;
-  size_t free_b = 0, total_b = 0;
-  GB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  const double budget = std::min<double>(24e9, 0.6 * (double)free_b);
+  const double budget = c.budget_or(24e9, 0.6);
   int kb = (int)std::max(1.0, std::floor(budget / (3.0 * (double)blk * sizeof(cplx))));
   kb = std::min(kb, nk);
   cplx* X1 = buf(SL_Y1, kb * blk);

@@ -138,9 +138,7 @@ static void hf_core(Context& c, const cplx* V, const cplx* dm, int nsp, int ndir
   // batch per k would leave most SMs idle); the per-k' partial results are then summed in k'
   // order by exchange_reduce_kernel, so the result is deterministic.
   const int64_t per_k = (int64_t)nsp * nk * pe;
-  size_t free_b = 0, total_b = 0;
-  GB_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  double budget = std::min<double>(8e9, 0.5 * (double)free_b);
+  const double budget = c.budget_or(8e9, 0.5);
   int kb = (int)std::max(1.0, std::floor(budget / ((double)per_k * sizeof(cplx))));
   kb = std::min(kb, nk);
   cplx* Y = (cplx*)c.scratch.get(SL_HF_Y, (size_t)kb * per_k * sizeof(cplx));

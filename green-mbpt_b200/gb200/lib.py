@@ -61,7 +61,7 @@ EXPORTED = [
     "gb200_iteration_device", "gb200_last_timings", "gb200_set_split_engine", "gb200_set_integrals_device",
     "gb200_set_q_range", "gb200_dyson_solve_device", "gb200_energy_device", "gb200_stats_enable", "gb200_stats_read",
     "gb200_hf_fock_noalloc", "gb200_set_q0_correction", "gb200_gw_sigma_vjp", "gb200_gw_sigma_vjp_device",
-    "gb200_set_contraction_slices",
+    "gb200_set_contraction_slices", "gb200_set_memory_budget",
 ]
 
 
@@ -99,6 +99,7 @@ def load(path: str | None = None):
     L.gb200_gw_sigma_device.argtypes = [vp, vp, vp, vp]
     L.gb200_gw_sigma_vjp.argtypes = [vp, vp, vp, vp, vp]
     L.gb200_set_contraction_slices.argtypes = [vp, vp]
+    L.gb200_set_memory_budget.argtypes = [vp, ctypes.c_double]
     L.gb200_gw_sigma_vjp_device.argtypes = [vp, vp, vp, vp, vp, vp]
     L.gb200_hf_fock.argtypes = [vp, vp, vp, ctypes.c_double, vp]
     L.gb200_hf_fock_device.argtypes = [vp, vp, vp, ctypes.c_double, vp, vp]
@@ -208,6 +209,10 @@ class Context:
             raise ValueError("six slice counts: P0 (a)-(c), Sigma (d)-(f)")
         arr = (ctypes.c_int * 6)(*[int(x) for x in slices])
         self._check(self._L.gb200_set_contraction_slices(self._h, arr))
+
+    def set_memory_budget(self, nbytes: float):
+        """Bytes the blocked intermediates of one call may use (0: a share of the free memory)."""
+        self._check(self._L.gb200_set_memory_budget(self._h, float(nbytes)))
 
     def set_split_engine(self, engine: int):
         """0: tcgen05 tensor cores, 1: CUDA-core validation engine (bit-identical INT32 sums)."""

@@ -120,6 +120,12 @@ int gb200_set_precision(gb200_context* ctx, int mode, int slices);
  * NULL resets all six to 0.  No counterpart in the reference (which runs FP64). */
 int gb200_set_contraction_slices(gb200_context* ctx, const int* slices6);
 
+/* Bytes the blocked intermediates of one call may use (the k-block buffers of the GW self-energy
+ * and its adjoint, the exchange intermediates of the Fock build); 0 (the default) takes a share of
+ * the free device memory at the call.  For several contexts sharing one GPU.  The reference sizes
+ * its buffers per MPI rank instead (gw_cpu_kernel.cpp:74-134); no counterpart. */
+int gb200_set_memory_budget(gb200_context* ctx, double bytes);
+
 /* GW self-energy: Sigma(tau,k) from G(tau,k), both [nts, ns, nk, nso, nso].
  * Replaces gw_cpu_kernel::solve (gw_cpu_kernel.cpp:31-72): Sigma is zeroed,
  * accumulated over q and divided by nk. */

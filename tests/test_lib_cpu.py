@@ -61,6 +61,7 @@ def test_null_context_is_an_error():
     L = lib.load()
     assert L.gb200_gw_sigma(None, None, None) == lib.ERR_INVALID
     assert L.gb200_set_contraction_slices(None, None) == lib.ERR_INVALID
+    assert L.gb200_set_memory_budget(None, 1e9) == lib.ERR_INVALID
     assert L.gb200_gw_sigma_vjp(None, None, None, None, None) == lib.ERR_INVALID
     t = (ctypes.c_float * 4)()
     assert L.gb200_last_timings(None, t) == lib.ERR_INVALID

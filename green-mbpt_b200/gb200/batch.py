@@ -29,6 +29,20 @@ class SystemBatch:
     def __len__(self):
         return len(self.contexts)
 
+    def share_memory(self, total_bytes: float):
+        """Give every context a budget for its blocked intermediates out of `total_bytes`, in
+        proportion to the size of one k-point block of its self-energy intermediates
+        (nts * ns * NQ * nao^2 complex values), so that all contexts fit on one GPU together."""
+        sizes = []
+        for c in self.contexts:
+            d = c.dims
+            sizes.append(float(d.nts) * d.ns * d.NQ * d.nao * d.nao * 16.0)
+        tot = sum(sizes)
+        budgets = [total_bytes * x / tot for x in sizes]
+        for c, b in zip(self.contexts, budgets):
+            c.set_memory_budget(b)
+        return budgets
+
     def run_gw(self, G_ptrs, Sigma_ptrs):
         """gw_sigma_device for every system (device pointers), concurrently; returns the per-system
         stage timings (ms) of the calls."""

@@ -72,3 +72,27 @@ def test_sharded_sigma_sums_to_full(tmp_path, name, ws):
     s = system(name)
     full = O.gw_solve(s.G, O.HalfStoredIntegrals(s.V_half), O.NoSymBZ(s.mesh), s.grid.Tnt_b, s.grid.Ttn_b, s.ns, s.NQ)
     assert np.abs(got - full).max() <= 1e-12 * np.abs(full).max()
+
+
+def test_batch_memory_shares_are_proportional():
+    """SystemBatch.share_memory splits a byte budget over contexts by their intermediate sizes."""
+    from gb200 import batch
+
+    class Dims:
+        def __init__(self, nts, ns, NQ, nao):
+            self.nts, self.ns, self.NQ, self.nao = nts, ns, NQ, nao
+
+    class Ctx:
+        def __init__(self, *d):
+            self.dims = Dims(*d)
+            self.budget = None
+
+        def set_memory_budget(self, b):
+            self.budget = b
+
+    ctxs = [Ctx(80, 1, 40, 8), Ctx(80, 1, 240, 48), Ctx(80, 2, 100, 20)]
+    b = batch.SystemBatch(ctxs).share_memory(60e9)
+    assert abs(sum(b) - 60e9) < 1.0
+    sizes = [80 * 1 * 40 * 64, 80 * 1 * 240 * 48 * 48, 80 * 2 * 100 * 400]
+    for c, x in zip(ctxs, sizes):
+        assert abs(c.budget / 60e9 - x / sum(sizes)) < 1e-12

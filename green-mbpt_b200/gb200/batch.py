@@ -71,10 +71,12 @@ class SystemBatch:
         self.contexts = []
 
 
-def uneven_systems(count: int = 16, seed: int = 0, nts: int = 80, beta: float = 100.0, meshes=None):
+def uneven_systems(count: int = 16, seed: int = 0, nts: int = 80, beta: float = 100.0, meshes=None,
+                   with_integrals: bool = True):
     """Synthetic systems of the batched workload: nk from {8, 27, 64}, nao ~ U{8..48},
     naux ~ U{4 nao .. 6 nao}, ntau = 80, beta = 100, per-system seeds (the generator of the
-    single-system configurations)."""
+    single-system configurations).  with_integrals=False leaves V out (to be generated on the
+    device, synth.upload_device_integrals)."""
     from . import synth
     rng = np.random.default_rng(seed)
     meshes = meshes or [(2, 2, 2), (3, 3, 3), (4, 4, 4)]
@@ -84,5 +86,5 @@ def uneven_systems(count: int = 16, seed: int = 0, nts: int = 80, beta: float = 
         nao = int(rng.integers(8, 49))
         naux = int(rng.integers(4 * nao, 6 * nao + 1))
         out.append(synth.make_system(mesh=mesh, nao=nao, naux=naux, ns=1, beta=beta, nts=nts, eps_range=2.0,
-                                     seed=seed * 1000 + i))
+                                     seed=seed * 1000 + i, with_integrals=with_integrals))
     return out

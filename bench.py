@@ -541,8 +541,9 @@ def main_batch(args):
         c.set_precision(lib.PREC_SPLIT, args.slices)
         ctxs.append(c)
     b = batch.SystemBatch(ctxs)
+    # budgets cover the k-block intermediates; their INT8 planes take about 2S/16 of that again
     free_b, _ = torch.cuda.mem_get_info(0)
-    b.share_memory(0.5 * free_b)
+    b.share_memory(0.4 * free_b)
     G = [torch.from_numpy(s.G).cuda() for s in systems]
     Sig = [torch.empty_like(x) for x in G]
     gp, sp = [x.data_ptr() for x in G], [x.data_ptr() for x in Sig]

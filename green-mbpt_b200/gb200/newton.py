@@ -153,15 +153,25 @@ def newton_krylov(phi, G0: torch.Tensor, steps: int, rtol: float = 1e-3, restart
         d, _, used = gmres(matvec, R, rtol=eta, restart=restart, maxiter=maxiter)
         hist.krylov.append(used)
         lam = 1.0
+        Gt = PGt = Rt = None
+        rt = math.inf
         for _ in range(max_backtracks + 1):
             Gt = G + lam * d
-            PGt = phi(Gt)
+            try:
+                PGt = phi(Gt)
+            except RuntimeError:
+                # a trial point the iteration cannot take (e.g. the chemical-potential search fails
+                # for an unphysical G far from the solution) counts as a rejected step
+                PGt = None
             evals += 1
-            Rt = PGt - Gt
-            rt = _norm(Rt)
-            if rt < (1.0 - 1e-4 * lam) * rn:
-                break
+            if PGt is not None:
+                Rt = PGt - Gt
+                rt = _norm(Rt)
+                if rt < (1.0 - 1e-4 * lam) * rn:
+                    break
             lam *= 0.5
+        if PGt is None:
+            raise RuntimeError("newton_krylov: no admissible step along the Newton direction")
         rn_prev = rn
         G, PG, R, rn = Gt, PGt, Rt, rt
     else:

@@ -103,3 +103,22 @@ def test_autograd_rejects_wrong_inputs_without_gpu():
         autograd.gw_sigma(c, torch.zeros(c.shape_G, dtype=torch.complex128))          # not on a GPU
     with pytest.raises(TypeError):
         autograd.gw_sigma(c, torch.zeros(c.shape_G, dtype=torch.complex64))
+
+
+def test_newton_krylov_rejects_steps_the_map_cannot_take():
+    """A map that fails (raises) outside |x| <= 1.5, and whose full Newton step from x0 lands there
+    (R(x) = -atan(x), the classic overshoot): the line search halves the step instead of aborting,
+    and the solve converges."""
+    raised = []
+
+    def phi(x):
+        if float(torch.abs(x).max()) > 1.5:
+            raised.append(1)
+            raise RuntimeError("outside the admissible region")
+        return x - torch.atan(x)
+
+    x0 = torch.tensor([1.45 + 0.0j, -1.45 + 0.0j], dtype=torch.complex128)
+    x, hist = newton.newton_krylov(phi, x0, steps=12, atol=1e-12, presteps=0)
+    assert raised
+    assert hist.residual[-1] < 1e-10
+    assert float(torch.abs(x).max()) < 1e-9

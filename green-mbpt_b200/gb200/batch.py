@@ -13,8 +13,6 @@ import concurrent.futures as cf
 
 import numpy as np
 
-from . import lib
-
 
 class SystemBatch:
     """A set of prepared contexts that are evaluated together."""

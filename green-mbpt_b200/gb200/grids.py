@@ -28,7 +28,6 @@ from __future__ import annotations
 import functools
 
 import numpy as np
-import scipy.linalg as sla
 
 
 def _chebyshev_nodes(nts: int, beta: float):

@@ -5,7 +5,6 @@ import numpy as np
 
 import gw_oracle as O
 from gb200 import synth
-from gb200.grids import ChebyshevGrid
 
 SMALL = dict(mesh=(2, 2, 1), nao=6, naux=20, ns=1, beta=20.0, nts=20, eps_range=2.0)
 SMALL_NS2 = dict(mesh=(2, 1, 2), nao=5, naux=16, ns=2, beta=20.0, nts=24, eps_range=2.0)

@@ -6,7 +6,6 @@ import re
 import shutil
 import subprocess
 
-import numpy as np
 import pytest
 
 from gb200 import lib

@@ -409,6 +409,15 @@ def main_ours(args):
             "clocks": r["clocks"], "gpu_launches": r["launches"],
             "energies": {"E_1b": r["E"][0], "E_HF": r["E"][1], "E_corr": r["E"][2], "mu": r["mu"]} if r["E"] else None,
         }
+        # size-independent properties of the full-size result: the new G(tau, k) is Hermitian (nothing
+        # enforces it: the Dyson step hermitizes Sigma, dyson.cpp:196-198, not G) and G, Sigma are finite
+        try:
+            def herm_dev(x):
+                return float((x - x.conj().transpose(-1, -2)).abs().max() / x.abs().max().clamp_min(1e-300))
+            line["properties"] = {"G_hermiticity_rel": herm_dev(r["G"]),
+                                  "finite": bool(r["St"].isfinite().all() and r["G"].isfinite().all())}
+        except Exception as ex:  # a report, not the measurement
+            line["properties"] = {"error": f"{type(ex).__name__}: {ex}"}
         # Chebyshev resolution of the new G (transformer_t::check_chebyshev's diagnostic): the
         # grid is the same for the GPU path and the oracle, so this does not affect parity
         try:

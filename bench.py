@@ -414,8 +414,9 @@ def main_ours(args):
         try:
             def herm_dev(x):
                 return float((x - x.conj().transpose(-1, -2)).abs().max() / x.abs().max().clamp_min(1e-300))
-            line["properties"] = {"G_hermiticity_rel": herm_dev(r["G"]),
-                                  "finite": bool(r["St"].isfinite().all() and r["G"].isfinite().all())}
+            Gnew = r["Gout"]  # the new G of the last timed step (the device copy is reused by the FP64 sample)
+            line["properties"] = {"G_hermiticity_rel": herm_dev(Gnew),
+                                  "finite": bool(r["St"].isfinite().all() and Gnew.isfinite().all())}
         except Exception as ex:  # a report, not the measurement
             line["properties"] = {"error": f"{type(ex).__name__}: {ex}"}
         # Chebyshev resolution of the new G (transformer_t::check_chebyshev's diagnostic): the

@@ -65,3 +65,23 @@ def test_full_sigma_within_bound_on_workload_shapes(gpu):
             out[name] = (G.cpu().numpy(), Sig.cpu().numpy())
     assert np.abs(out["split"][1] - out["fp64"][1]).max() <= 1e-8
     assert np.abs(out["split"][0] - out["fp64"][0]).max() <= 1e-8
+
+
+@pytest.mark.parametrize("name", ["small", "small_ns2"])
+def test_split_matches_cpu_model_of_its_arithmetic(gpu, name):
+    """The GPU split engine against oracle/split_model.py, the CPU restatement of its arithmetic
+    (exponents per row and column with one bit of headroom, rounded balanced base-128 digits, kept
+    diagonals), at three slices.  On these systems all k-points form one block and no contraction
+    is chunked, so both form the same exponent groups and the same exact integer digit products:
+    they agree to 1e-10 relative, while both differ from the FP64 result by about 1e-6 relative and
+    truncated digits would differ from balanced ones by as much.  (Three slices: the digit quantum,
+    2^-21 of the row maximum, is far above the FP64 round-off in which the two differ, so no
+    rounding decision of a later contraction's slicing flips between them.)"""
+    import split_model as SM
+    s = system(name)
+    model = SM.gw_split_model(s, {c: 3 for c in "abcdef"})
+    with solvers.make_context(s, precision=lib.PREC_SPLIT, slices=3) as c:
+        got = c.gw_sigma(s.G)
+    scale = np.abs(model).max()
+    assert np.abs(got - model).max() <= 1e-10 * scale
+    assert np.abs(model - oracle_sigma(name)).max() > 1e-8 * scale

@@ -179,6 +179,8 @@ void gb200_destroy(gb200_context* ctx) {
   }
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : c->qev)
+    if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -227,7 +229,6 @@ int gb200_set_integrals(gb200_context* ctx, int which, const double* V_half, int
     if (which == GB200_INTEGRALS_GW) {
       upload_integrals(c, c.V, V_half, npairs, false, c.stream);
       c.have_V = true;
-      split_invalidate(c);
     } else if (which == GB200_INTEGRALS_HF) {
       upload_integrals(c, c.Vhf, V_half, npairs, false, c.stream);
       c.have_Vhf = true;
@@ -242,7 +243,6 @@ int gb200_set_precision(gb200_context* ctx, int mode, int slices) {
     require(mode == GB200_PREC_FP64 || mode == GB200_PREC_SPLIT, GB200_ERR_INVALID, "set_precision: unknown mode");
     if (mode == GB200_PREC_SPLIT)
       require(slices >= 2 && slices <= 8, GB200_ERR_INVALID, "set_precision: slices must be in [2, 8]");
-    if (mode != c.prec_mode || slices != c.slices) split_invalidate(c);
     c.prec_mode = mode;
     c.slices = slices;
   });
@@ -484,7 +484,6 @@ int gb200_set_integrals_device(gb200_context* ctx, int which, const double* V_de
     done += pair_count;
     if (which == GB200_INTEGRALS_GW) {
       c.have_V = done >= npairs;
-      split_invalidate(c);
     } else {
       c.have_Vhf = done >= npairs;
     }

@@ -125,6 +125,8 @@ struct Context {
   std::vector<KernelRecord> records;
   size_t records_used = 0;
   cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  // stage boundaries of the GW q loop (4 per q-point), read once after the loop
+  std::vector<cudaEvent_t> qev;
 
   int64_t nao() const { return d.nao; }
   int64_t pair_elems() const { return (int64_t)d.NQ * d.nao * d.nao; }

@@ -316,7 +316,6 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
   cplx* X1 = (cplx*)c.scratch.get(SL_Y1, (size_t)kb * per_k_sigma * sizeof(cplx));
   cplx* X2 = (cplx*)c.scratch.get(SL_Y2, (size_t)kb * per_k_sigma * sizeof(cplx));
   SplitEngine* se = split ? split_engine(c) : nullptr;
-  if (se) split_prepare_integrals(c, *se, st);
   // the P0 and Sigma contractions run in the selected precision; the
   // transforms and the aux-basis solve always run in FP64
   auto contract = [&](const ZGemm& g, int stage) {
@@ -334,9 +333,18 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
   // the partial Sigma is already divided by nk, so shards sum to the full self-energy
   const int q0 = std::max(0, c.q_begin);
   const int q1 = c.q_end < 0 ? nk : std::min(nk, c.q_end);
+  // stage timings: events recorded on the stream and read after the loop, so the host never
+  // waits inside it
+  const size_t nev = (size_t)std::max(0, q1 - q0) * 4;
+  while (c.qev.size() < nev) {
+    cudaEvent_t e;
+    GB_CUDA(cudaEventCreate(&e));
+    c.qev.push_back(e);
+  }
   for (int q = q0; q < q1; ++q) {
+    cudaEvent_t* qe = c.qev.data() + (size_t)(q - q0) * 4;
     // ---------------- polarization P0(tau, q), tau in the first half ---------
-    GB_CUDA(cudaEventRecord(c.ev[1], st));
+    GB_CUDA(cudaEventRecord(qe[0], st));
     GB_CUDA(cudaMemsetAsync(P0, 0, (size_t)nts * NQ * NQ * sizeof(cplx), st));
     for (int k0 = 0; k0 < nk; k0 += kb) {
       const int kbk = std::min(kb, nk - k0);
@@ -384,7 +392,7 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
       symmetrize_p0_kernel<<<grid_for(total, 256), 256, 0, st>>>(P0, nts, NQ, 1.0 / nk);
       GB_CHECK_LAUNCH();
     }
-    GB_CUDA(cudaEventRecord(c.ev[2], st));
+    GB_CUDA(cudaEventRecord(qe[1], st));
     // ---------------- screened interaction (gw_cpu_kernel.cpp:227-279) -------
     {
       ZGemm f;  // Pw[n] = sum_t Tnt_b[n][t] P0[t]
@@ -427,7 +435,7 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
       bt.C.ptr = P0; bt.C.row = lin((int64_t)NQ * NQ); bt.C.col = lin(1);
       zgemm_fp64(bt, st);
     }
-    GB_CUDA(cudaEventRecord(c.ev[3], st));
+    GB_CUDA(cudaEventRecord(qe[2], st));
     // ---------------- self-energy contribution of this q ---------------------
     for (int k0 = 0; k0 < nk; k0 += kb) {
       const int kbk = std::min(kb, nk - k0);
@@ -470,13 +478,7 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
       contract(e, 4);
       contract(f, 5);
     }
-    GB_CUDA(cudaEventRecord(c.ev[4], st));
-    GB_CUDA(cudaEventSynchronize(c.ev[4]));
-    float a_ms = 0, b_ms = 0, c_ms = 0;
-    GB_CUDA(cudaEventElapsedTime(&a_ms, c.ev[1], c.ev[2]));
-    GB_CUDA(cudaEventElapsedTime(&b_ms, c.ev[2], c.ev[3]));
-    GB_CUDA(cudaEventElapsedTime(&c_ms, c.ev[3], c.ev[4]));
-    t_p0 += a_ms; t_w += b_ms; t_sig += c_ms;
+    GB_CUDA(cudaEventRecord(qe[3], st));
   }
   scale_inplace(Sigma, (int64_t)nts * ns * nk * nao2, 1.0 / nk, st);  // gw_cpu_kernel.cpp:55
   if (x2c) {
@@ -493,6 +495,14 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
   GB_CUDA(cudaEventSynchronize(c.ev[4]));
   float tot = 0;
   GB_CUDA(cudaEventElapsedTime(&tot, c.ev[0], c.ev[4]));
+  for (int q = q0; q < q1; ++q) {
+    const cudaEvent_t* qe = c.qev.data() + (size_t)(q - q0) * 4;
+    float a_ms = 0, b_ms = 0, c_ms = 0;
+    GB_CUDA(cudaEventElapsedTime(&a_ms, qe[0], qe[1]));
+    GB_CUDA(cudaEventElapsedTime(&b_ms, qe[1], qe[2]));
+    GB_CUDA(cudaEventElapsedTime(&c_ms, qe[2], qe[3]));
+    t_p0 += a_ms; t_w += b_ms; t_sig += c_ms;
+  }
   c.timings[0] = t_p0; c.timings[1] = t_w; c.timings[2] = t_sig; c.timings[3] = tot;
 }
 

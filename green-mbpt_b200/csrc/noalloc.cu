@@ -10,15 +10,20 @@
 //
 // The computation is the one of gb200_hf_fock_device (hf_cpu_kernels.cpp:25-146)
 // with the exchange term taken one k at a time so that its intermediate fits the
-// fixed workspace.  The first call on a device looks up the array's device
-// address with cudaGetSymbolAddress (once per device, with that device
-// current), so that first call should come before any stream capture.  All
-// calls share the array and it keeps the contents of the last call: calls that
-// overlap on the GPU (two streams, two host threads) race on it.
+// fixed workspace.  Only scalar input (nso = nao) is accepted.  Host code cannot
+// use the array's name as a device address, so each call looks the address up
+// with cudaGetSymbolAddress for the current device and context.  While the
+// stream is being captured into a graph the address recorded by an earlier call
+// in the same context is used instead, so the first call in a context should
+// come before any stream capture.  All calls share the array and it keeps the
+// contents of the last call: calls that overlap on the GPU (two streams, two
+// host threads) race on it.
 #include <algorithm>
 #include <cstdio>
 #include <mutex>
 #include <string>
+
+#include <cuda.h>
 
 #include "context.cuh"
 
@@ -29,22 +34,59 @@ namespace {
 constexpr size_t NOALLOC_SCRATCH_BYTES = 64ull << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
+// Address of the workspace per (device, context).  A context that was destroyed
+// (cudaDeviceReset) and recreated loads the module again, possibly at another
+// address, so the cached value is refreshed on every call that is not being
+// captured and is only trusted while a capture is in progress.
 constexpr int MAX_DEVICES = 64;
 std::mutex g_addr_mutex;
-void* g_addr[MAX_DEVICES] = {nullptr};
+struct AddrEntry {
+  CUcontext ctx = nullptr;
+  void* ptr = nullptr;
+};
+AddrEntry g_addr[MAX_DEVICES];
 
-// Device address of the workspace on the current device (looked up once per device).
-void* scratch_address(int dev) {
+// cuCtxGetCurrent through the runtime's driver entry point, so the library has no link-time
+// dependency on the driver library
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrentFn>(f);
+  });
+  require(fn != nullptr, GB200_ERR_CUDA, "hf_fock_noalloc: cuCtxGetCurrent unavailable");
+  return fn;
+}
+
+void* scratch_address(int dev, cudaStream_t st) {
   require(dev >= 0 && dev < MAX_DEVICES, GB200_ERR_INVALID, "hf_fock_noalloc: device index out of range");
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  GB_CUDA(cudaStreamIsCapturing(st, &cap));
   std::lock_guard<std::mutex> lk(g_addr_mutex);
-  if (!g_addr[dev]) {
-    void* p = nullptr;
+  AddrEntry& ent = g_addr[dev];
+  void* p = nullptr;
+  if (cap == cudaStreamCaptureStatusNone) {
+    // the lookup also makes the device's context current if it was not yet
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     require(e == cudaSuccess && p != nullptr, GB200_ERR_CUDA,
             std::string("hf_fock_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
-    g_addr[dev] = p;
   }
-  return g_addr[dev];
+  CUcontext cur = nullptr;
+  require(ctx_get_current()(&cur) == CUDA_SUCCESS && cur != nullptr, GB200_ERR_CUDA,
+          "hf_fock_noalloc: no current CUDA context");
+  if (cap != cudaStreamCaptureStatusNone) {
+    require(ent.ctx == cur && ent.ptr != nullptr, GB200_ERR_STATE,
+            "hf_fock_noalloc: the first call in this context must come before stream capture");
+    return ent.ptr;
+  }
+  ent.ctx = cur;
+  ent.ptr = p;
+  return p;
 }
 
 __host__ __device__ inline size_t align256(size_t b) { return (b + 255) / 256 * 256; }
@@ -117,19 +159,22 @@ extern "C" int gb200_hf_fock_noalloc(const gb200_dims* dims, const double* V_dev
     const gb200_dims d = *dims;
     require(d.nk > 0 && d.nao > 0 && d.NQ > 0 && (d.ns == 1 || d.ns == 2), GB200_ERR_INVALID,
             "hf_fock_noalloc: need nk, nao, NQ > 0 and ns in {1, 2}");
+    require(d.nso == 0 || d.nso == d.nao, GB200_ERR_INVALID,
+            "hf_fock_noalloc: two-component input (nso = 2*nao) is not supported; only nso = nao (or 0)");
     const NoallocPlan p = plan_noalloc(d);
     if (p.kpb < 1) {
-      char msg[320];
+      char msg[400];
       std::snprintf(msg, sizeof msg,
                     "hf_fock_noalloc: sizes need %zu bytes of workspace, above the fixed maximum of %zu bytes "
-                    "(2*ns*nk*nao^2 + ns*NQ*nao^2 complex numbers must fit); use gb200_hf_fock_device",
+                    "(16 * (ns*nk*nao^2 + max(ns*NQ*nao^2, ns*nk*nao^2)) bytes plus small tables must fit); "
+                    "use gb200_hf_fock_device",
                     p.total, NOALLOC_SCRATCH_BYTES);
       throw Error(GB200_ERR_INVALID, msg);
     }
     int dev = 0;
     GB_CUDA(cudaGetDevice(&dev));
-    unsigned char* base = static_cast<unsigned char*>(scratch_address(dev));
     cudaStream_t st = (cudaStream_t)stream;
+    unsigned char* base = static_cast<unsigned char*>(scratch_address(dev, st));
 
     const cplx* V = reinterpret_cast<const cplx*>(V_dev);
     const cplx* dm = reinterpret_cast<const cplx*>(dm_dev);

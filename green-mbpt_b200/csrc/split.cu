@@ -889,10 +889,6 @@ SplitEngine* split_engine(Context& c) {
   return c.split;
 }
 
-void split_prepare_integrals(Context&, SplitEngine&, cudaStream_t) {}
-
-void split_invalidate(Context&) {}
-
 void split_release(Context& c) {
   delete c.split;
   c.split = nullptr;

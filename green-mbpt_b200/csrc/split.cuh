@@ -9,14 +9,10 @@ struct SplitEngine;
 
 // The engine of a context (created on first use).
 SplitEngine* split_engine(Context& c);
-// Prepare per-integral data (no-op when nothing is cached).
-void split_prepare_integrals(Context& c, SplitEngine& se, cudaStream_t st);
 // C = alpha op(A) op(B) + beta C with both operands sliced into INT8 pieces,
 // products on the tensor cores with exact INT32 accumulation, FP64 recombination;
 // `slices` pieces per operand (0: the context's count).
 void split_gemm(Context& c, SplitEngine& se, const ZGemm& g, cudaStream_t st, int slices = 0);
-// Drop cached slices (integrals or precision changed).
-void split_invalidate(Context& c);
 void split_release(Context& c);
 // Non-zero if a split kernel hit a bounded-wait timeout since the last check (flag is cleared).
 int split_check_error(Context& c, cudaStream_t st);

@@ -158,18 +158,21 @@ int gb200_hf_fock_device(gb200_context* ctx, const double* dm_dev, const double*
  * holds the free HBM, or that must avoid the device-wide synchronisation of
  * cudaMalloc/cudaFree.  No counterpart in the reference.  It needs no context
  * and calls no allocating routine: the caller passes the dimensions (dims->nk,
- * nao, ns, NQ are read), the full-storage integrals V_dev [nk][nk][NQ][nao][nao]
+ * nao, ns, NQ are read; dims->nso must be 0 or nao, since two-component input
+ * is rejected with GB200_ERR_INVALID), the full-storage integrals V_dev [nk][nk][NQ][nao][nao]
  * (complex128, pair (k,k') at ((k*nk + k')*NQ)*nao*nao), dm_dev, S_dev and
  * F_dev [ns][nk][nao][nao], and a stream (NULL = legacy default stream).
  * Working memory is one fixed 64 MiB device array inside the library, which
  * every GPU that loads the library holds until the process exits.  Sizes whose
- * workspace, 16 * (2*ns*nk*nao^2 + ns*NQ*nao^2) bytes plus small tables, does
- * not fit are rejected with GB200_ERR_INVALID and a message readable through
- * gb200_last_error(NULL).  The first call on a device looks up that array's
- * address for the device (once), so make it before any stream capture.  Every
- * call shares the array and its contents stay from the last call: calls that
- * overlap on the GPU (different streams or host threads) race.  The call is
- * asynchronous on `stream`. */
+ * workspace, 16 * (ns*nk*nao^2 + max(ns*NQ*nao^2, ns*nk*nao^2)) bytes plus small
+ * tables, does not fit are rejected with GB200_ERR_INVALID and a message
+ * readable through gb200_last_error(NULL).  Each call looks up that array's
+ * address for the current device and context; while `stream` is being captured
+ * it reuses the address an earlier call in the same context found, so make the
+ * first call in a context before any stream capture.  Every call shares the
+ * array and its contents stay from the last call: calls that overlap on the GPU
+ * (different streams or host threads) race.  The call is asynchronous on
+ * `stream`. */
 int gb200_hf_fock_noalloc(const gb200_dims* dims, const double* V_dev, const double* dm_dev, const double* S_dev,
                           double madelung, double* F_dev, void* stream);
 

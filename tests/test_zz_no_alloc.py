@@ -53,7 +53,8 @@ def _case_small(name):
 
 
 def _case_blocked():
-    """nk = 9, nao = 32, NQ = 400, ns = 2: the exchange work area holds 4 of the 9 k' at once."""
+    """nk = 9, nao = 32, NQ = 400, ns = 2: the exchange work area holds 5 of the 9 k' at once, so the
+    exchange term runs in two blocks of k' (5 and 4)."""
     mesh, nao, NQ, ns = (3, 3, 1), 32, 400, 2
     nk = 9
     rng = np.random.default_rng(5)
@@ -101,6 +102,37 @@ def test_noalloc_matches_device_entry_point(gpu, case):
         assert np.isfinite(g).all()
         assert rel(g, w) < TOL, (case, i, rel(g, w))
     assert rel(want[1].cpu().numpy(), want[0].cpu().numpy()) > 1e-6  # the two calls had different inputs
+
+
+@pytest.mark.gpu
+def test_noalloc_matches_oracle(gpu):
+    """The allocation-free Fock build against the CPU oracle's restatement of hf_scalar_cpu_kernel, with a
+    nonzero Madelung constant, on the spin-polarised small system."""
+    import torch
+    from _systems import oracle_fock
+    s = system("small_ns2")
+    madelung = 0.37
+    want = oracle_fock(s, madelung)
+    pref = -1.0 if s.ns == 2 else -2.0
+    dm = torch.from_numpy(np.ascontiguousarray(pref * s.G[-1])).cuda()
+    V = _full_from_half(s.V_half, s.nk)
+    S_d = torch.from_numpy(np.ascontiguousarray(s.S)).cuda()
+    F = torch.full_like(dm, float("nan"))
+    stream = torch.cuda.current_stream().cuda_stream
+    lib.hf_fock_noalloc(s.nk, s.nao, s.ns, s.NQ, V.data_ptr(), dm.data_ptr(), S_d.data_ptr(), madelung,
+                        F.data_ptr(), stream)
+    torch.cuda.synchronize()
+    assert rel(F.cpu().numpy(), want) < TOL
+
+
+def test_noalloc_rejects_two_component_input():
+    """Two-component dimensions (nso = 2 nao) fail with GB200_ERR_INVALID before any device work."""
+    L = lib.load()
+    d = lib.Dims(4, 3, 6, 1, 10, 0, 0, 0, 0.0)
+    fake = ctypes.c_void_p(256)  # never dereferenced: the dimension check comes first
+    rc = L.gb200_hf_fock_noalloc(ctypes.byref(d), fake, fake, fake, 0.0, fake, None)
+    assert rc == lib.ERR_INVALID
+    assert "two-component" in L.gb200_last_error(None).decode()
 
 
 def test_noalloc_rejects_sizes_beyond_the_workspace():

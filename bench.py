@@ -192,7 +192,7 @@ def blas_threads():
         return os.cpu_count()
 
 
-def setup_context(cfg, seed, slices, device, ws, rank, contraction_slices=None):
+def setup_context(cfg, seed, slices, device, ws, rank, contraction_slices=None, engine=0):
     from gb200 import lib, shard, solvers, synth
 
     s = synth.make_config(cfg, seed=seed, with_integrals=False)
@@ -204,6 +204,7 @@ def setup_context(cfg, seed, slices, device, ws, rank, contraction_slices=None):
     synth.upload_device_integrals(ctx, s.nk, s.NQ, s.nao, seed=seed, device=device)
     ctx.set_hamiltonian(s.F, s.S)
     ctx.set_precision(lib.PREC_SPLIT, slices)
+    ctx.set_split_engine(engine)
     if contraction_slices:
         ctx.set_contraction_slices(contraction_slices)
     if ws > 1:
@@ -223,7 +224,8 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(minutes=15))
     from gb200 import lib, shard
 
-    s, ctx = setup_context(args.config, args.seed, args.slices, local, ws, rank, args.contraction_slices)
+    s, ctx = setup_context(args.config, args.seed, args.slices, local, ws, rank, args.contraction_slices,
+                           args.engine)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
     # the library runs on torch's stream, so its work is ordered with the copies around it; a null
@@ -465,7 +467,7 @@ def main_gw_profile(args):
     import torch
 
     torch.cuda.set_device(0)
-    s, ctx = setup_context(args.config, args.seed, args.slices, 0, 1, 0, args.contraction_slices)
+    s, ctx = setup_context(args.config, args.seed, args.slices, 0, 1, 0, args.contraction_slices, args.engine)
     G = torch.from_numpy(s.G).cuda()
     Sig = torch.empty_like(G)
     ctx.set_q_range(0, min(args.gw_q, s.nk))
@@ -643,6 +645,8 @@ def parse(argv=None):
                     help="slices of the six contractions P0 (a)-(c), Sigma (d)-(f), comma-separated; "
                          "0 keeps --slices")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--engine", type=int, default=0, choices=[0, 1],
+                    help="split engine: 0 tcgen05 tensor cores (default), 1 the CUDA-core validation engine")
     ap.add_argument("--no-fp64", dest="no_fp64", action="store_true",
                     help="skip the whole FP64 iteration (its time and the full-size split-vs-FP64 accuracy)")
     ap.add_argument("--gw-q", dest="gw_q", type=int, default=0,

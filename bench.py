@@ -468,6 +468,9 @@ def main_gw_profile(args):
 
     torch.cuda.set_device(0)
     s, ctx = setup_context(args.config, args.seed, args.slices, 0, 1, 0, args.contraction_slices, args.engine)
+    if args.profile_fp64:
+        from gb200 import lib
+        ctx.set_precision(lib.PREC_FP64, args.slices)
     G = torch.from_numpy(s.G).cuda()
     Sig = torch.empty_like(G)
     ctx.set_q_range(0, min(args.gw_q, s.nk))
@@ -482,7 +485,8 @@ def main_gw_profile(args):
     torch.cuda.synchronize()
     torch.cuda.profiler.stop()
     print(json.dumps({"profile_case": WORKLOADS[args.config], "q_points": min(args.gw_q, s.nk),
-                      "precision": f"split, {args.slices} INT8 slices", "stage_ms": out[-1]}), flush=True)
+                      "precision": "FP64" if args.profile_fp64 else f"split, {args.slices} INT8 slices",
+                      "stage_ms": out[-1]}), flush=True)
     ctx.close()
 
 
@@ -651,6 +655,8 @@ def parse(argv=None):
                     help="skip the whole FP64 iteration (its time and the full-size split-vs-FP64 accuracy)")
     ap.add_argument("--gw-q", dest="gw_q", type=int, default=0,
                     help="profiling case: time only the GW self-energy over q-points [0, GW_Q)")
+    ap.add_argument("--profile-fp64", dest="profile_fp64", action="store_true",
+                    help="profiling case in FP64 instead of split precision")
     ap.add_argument("--newton", type=int, default=0,
                     help="differentiable-step case (--config c4): adjoint timings, then N plain and N "
                          "Newton-Krylov self-consistency steps from the same start")

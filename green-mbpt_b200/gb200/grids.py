@@ -160,6 +160,100 @@ class ChebyshevGrid:
         return float(np.abs(c[-1]).max() / first) if first > 0 else 0.0
 
 
+def _omega_quadrature(wmax: float, beta: float, p: int = 64):
+    """Composite Gauss-Legendre nodes and weights on [-wmax, wmax], segments doubling in length from
+    |omega| = 1/(8 beta) outward (the kernels vary on the scale 1/beta near 0 and 1/tau_min far out)."""
+    edges = [0.0, 1.0 / (8.0 * beta)]
+    while edges[-1] < wmax:
+        edges.append(min(2.0 * edges[-1], wmax))
+    e = np.array(edges)
+    g, w = np.polynomial.legendre.leggauss(p)
+    X = ((e[:-1, None] + e[1:, None]) / 2 + (e[1:, None] - e[:-1, None]) / 2 * g).ravel()
+    W = ((e[1:, None] - e[:-1, None]) / 2 * w).ravel()
+    return np.concatenate([-X[::-1], X]), np.concatenate([W[::-1], W])
+
+
+def fermi_kernel_tau(tau, omega, beta):
+    """exp(-tau w) / (1 + exp(-beta w)) without overflow: [len(tau), len(omega)]."""
+    t, w = np.asarray(tau)[:, None], np.asarray(omega)[None, :]
+    pos = w >= 0
+    a = np.exp(-t * np.where(pos, w, 0.0)) / (1.0 + np.exp(-beta * np.where(pos, w, 0.0)))
+    wn = np.where(pos, 0.0, w)
+    b = np.exp((beta - t) * wn) / (1.0 + np.exp(beta * wn))
+    return np.where(pos, a, b)
+
+
+def bose_kernel_tau(tau, omega, beta):
+    """w exp(-tau w) / (1 - exp(-beta w)) (finite, 1/beta at w = 0) without overflow."""
+    t, w = np.asarray(tau)[:, None], np.asarray(omega)[None, :]
+    aw = np.abs(w)
+    small = aw * beta < 1e-12
+    wsafe = np.where(small, 1.0, w)
+    # w > 0: w e^{-t w} / (1 - e^{-beta w});  w < 0: |w| e^{(beta - t) w} / (1 - e^{beta w})
+    num = np.where(w > 0, np.exp(-t * np.where(w > 0, w, 0.0)), np.exp((beta - t) * np.where(w < 0, w, 0.0)))
+    den = -np.expm1(-beta * np.abs(wsafe))
+    out = np.abs(wsafe) * num / den
+    return np.where(small, 1.0 / beta, out)
+
+
+class SampledGrid:
+    """Transforms for given imaginary-time sampling points (for example the points of a green-grids
+    IR grid file, which green-mbpt's own result files record as the mesh of G_tau).
+
+    A function of tau is represented by its spectral form F(tau) = int K(tau, w) rho(w) dw over
+    |w| <= wmax, with the fermionic kernel exp(-tau w)/(1 + exp(-beta w)) or the bosonic one
+    w exp(-tau w)/(1 - exp(-beta w)) on a composite Gauss-Legendre w grid.  The Matsubara transform
+    of a kernel column is known in closed form (int_0^beta e^{i w_n tau} K dtau = 1/(w - i w_n), and
+    w/(w - i W_n) for bosons), so tau -> i w_n is (K_iw pinv(K_tau)) and i w_n -> tau is
+    (K_tau pinv(K_iw)), both pseudo-inverses truncated at `rcut` of the largest singular value and
+    applied through the singular vectors (never formed as matrices of size 1/s_min).
+    Functions whose spectra lie in the window are reproduced whatever frequencies are sampled, which
+    is what makes results on these points comparable with a calculation that used the IR basis of
+    the same window.  Sampling frequencies: every Matsubara index up to `ndense`, then geometrically
+    spaced ones up to about wmax * `wfac`, in conjugate pairs."""
+
+    def __init__(self, tau, beta: float, wmax: float, ndense: int = 128, ngeo: int = 64, wfac: float = 20.0,
+                 rcut: float = 1e-15):
+        tau = np.asarray(tau, dtype=np.float64)
+        if len(tau) % 2 != 0:
+            raise ValueError("Number of tau points should be even")
+        self.tau, self.beta, self.wmax = tau, float(beta), float(wmax)
+        self.nts = len(tau)
+        X, W = _omega_quadrature(self.wmax, self.beta)
+        sw = np.sqrt(W)
+        nmax = max(ndense + 1, int(np.ceil(self.wmax * wfac * self.beta / (2 * np.pi))))
+        geo = np.unique(np.round(np.geomspace(ndense + 1, nmax, ngeo)).astype(int))
+        pos = np.concatenate([np.arange(ndense + 1), geo[geo > ndense]])
+        # bosonic: 0 and +-n; fermionic: n >= 0 and their partners -n-1
+        self.n_b = np.concatenate([-pos[:0:-1], pos])
+        self.n_f = np.concatenate([-pos[::-1] - 1, pos])
+        self.wsample_b = 2 * np.pi * self.n_b / self.beta
+        self.wsample_f = (2 * self.n_f + 1) * np.pi / self.beta
+        self.nw, self.nw_b = len(self.n_f), len(self.n_b)
+
+        def apply_pinv(L, K):
+            # L pinv(K) grouped as ((L V) / s) U^H: L V ~ s (the transform's own basis) stays moderate,
+            # while pinv(K) alone has entries ~ 1 / s_min and would cancel catastrophically
+            U, S, Vh = np.linalg.svd(K, full_matrices=False)
+            r = int((S > rcut * S[0]).sum())
+            return ((L @ np.conj(Vh[:r]).T) / S[:r]) @ np.conj(U[:, :r]).T
+
+        def transforms(Ktau, Kiw):
+            Ktau, Kiw = Ktau * sw, Kiw * sw
+            return apply_pinv(Kiw, Ktau), apply_pinv(Ktau, Kiw)
+
+        Kf_iw = 1.0 / (X[None, :] - 1j * self.wsample_f[:, None])
+        self.Tnt_f, self.Ttn_f = transforms(fermi_kernel_tau(tau, X, self.beta), Kf_iw)
+        Wb = self.wsample_b[:, None]
+        Kb_iw = np.where(np.abs(X[None, :]) + np.abs(Wb) > 0, X[None, :] / (X[None, :] - 1j * Wb + (X[None, :] == 0) * (Wb == 0)), 1.0)
+        self.Tnt_b, self.Ttn_b = transforms(bose_kernel_tau(tau, X, self.beta), Kb_iw)
+
+    @property
+    def Ttn_beta(self):
+        """Row of Ttn at tau = beta (dyson.cpp:76, common_utils.cpp:16)."""
+        return self.Ttn_f[-1]
+
+
 @functools.lru_cache(maxsize=8)
 def cached_grid(beta: float, nts: int, nw: int | None = None, nw_b: int | None = None) -> ChebyshevGrid:
     return ChebyshevGrid(beta, nts, nw, nw_b)

@@ -62,6 +62,28 @@ def context_from_files(input_path: str, hf_integrals: str | None = None, gw_inte
     """
     from . import inputs
     inp = inputs.read_input(input_path)
+    npairs = len(inp["symmetry"].kpair_irre)
+    hf = inputs.read_integrals(hf_integrals, npairs)[0] if hf_integrals else None
+    gw = inputs.read_integrals(gw_integrals, npairs)[0] if gw_integrals else None
+    q0 = None
+    if q0_file:
+        from .h5lite import H5File
+        A, q_abs, _ = inputs.read_q0(q0_file)
+        q0 = (A, q_abs, np.asarray(H5File(input_path).read("symmetry/q/ibz2bz")))
+    return context_from_arrays(inp, hf, gw, grid, beta, device, q0)
+
+
+def context_from_arrays(inp: dict, hf_store=None, gw_store=None, grid=None, beta: float | None = None,
+                        device: int = 0, q0=None):
+    """The context of context_from_files from arrays already in memory.
+
+    inp: the dictionary of inputs.read_input (nk, nao, nso, ns, NQ, symmetry as an
+    inputs.KSymmetry, and optionally k_frac, S_ibz, H_ibz, madelung); hf_store / gw_store: the
+    irreducible k-pair blocks [npairs, NQ, nao, nao] of the integral files; q0: (AqQ, q_abs,
+    q_ibz2bz) at the irreducible q-points for the "extrapolate" q -> 0 correction.
+    Returns (context, inp) with the full-zone S and H added to inp.
+    """
+    from . import inputs
     sym = inp["symmetry"]
     nk, nao, nso, ns, NQ = inp["nk"], inp["nao"], inp["nso"], inp["ns"], inp["NQ"]
     if grid is not None:
@@ -70,28 +92,27 @@ def context_from_files(input_path: str, hf_integrals: str | None = None, gw_inte
         ctx.set_grid(grid.Tnt_f, grid.Ttn_f, grid.Tnt_b, grid.Ttn_b, grid.wsample_f)
     else:
         ctx = lib.Context(nk, nao, ns, NQ, 2, 2, 3, float(beta or 1.0), nso=nso, device=device)
-    if inp.get("k_frac") is not None:
-        kp, km = inputs.kq_maps_from_points(inp["k_frac"])
-        ctx.set_kq_maps(kp, km)
-    npairs = len(sym.kpair_irre)
-    if hf_integrals:
-        store, _ = inputs.read_integrals(hf_integrals, npairs)
-        ctx.set_integrals(sym.half_storage(store), lib.INTEGRALS_HF)
-    if gw_integrals:
-        store, _ = inputs.read_integrals(gw_integrals, npairs)
-        ctx.set_integrals(sym.half_storage(store), lib.INTEGRALS_GW)
-    if q0_file:
-        from .h5lite import H5File
-        A, q_abs, _ = inputs.read_q0(q0_file)
-        ibz2bz_q = np.asarray(H5File(input_path).read("symmetry/q/ibz2bz"))
-        Af, qf = inputs.q0_full_zone(A, q_abs, ibz2bz_q, nk)
-        ctx.set_q0_correction(Af, qf, inp["madelung"])
-    if "S_ibz" in inp:
-        inp["S"] = sym.full_from_ibz(inp["S_ibz"])
-    if "H_ibz" in inp:
-        inp["H"] = sym.full_from_ibz(inp["H_ibz"])
-        if "S" in inp:
-            ctx.set_hamiltonian(inp["H"], inp["S"])
+    try:
+        if inp.get("k_frac") is not None:
+            kp, km = inputs.kq_maps_from_points(inp["k_frac"])
+            ctx.set_kq_maps(kp, km)
+        if hf_store is not None:
+            ctx.set_integrals(sym.half_storage(hf_store), lib.INTEGRALS_HF)
+        if gw_store is not None:
+            ctx.set_integrals(sym.half_storage(gw_store), lib.INTEGRALS_GW)
+        if q0 is not None:
+            A, q_abs, ibz2bz_q = q0
+            Af, qf = inputs.q0_full_zone(A, q_abs, ibz2bz_q, nk)
+            ctx.set_q0_correction(Af, qf, inp.get("madelung", 0.0))
+        if "S_ibz" in inp:
+            inp["S"] = sym.full_from_ibz(inp["S_ibz"])
+        if "H_ibz" in inp:
+            inp["H"] = sym.full_from_ibz(inp["H_ibz"])
+            if "S" in inp:
+                ctx.set_hamiltonian(inp["H"], inp["S"])
+    except BaseException:
+        ctx.close()
+        raise
     return ctx, inp
 
 

@@ -15,12 +15,16 @@ Parity status
   symmetry (``RefSymmetry``) are pinned against the reference's own golden
   fixtures (test/data/HF, HF_X2C, HF_orth_invariance) at 1e-10 — see
   tests/test_oracle_golden.py.
-* The GW self-energy (P0 -> W -> Sigma) and the Dyson step follow the same
-  reference code, but the reference's GW fixtures need the IR grid file of the
-  external green-grids package (``ir/1e4.h5``), which is not available, so the
-  GW part is pinned only by identities (hermiticity, tau mirror symmetry,
-  basis-rotation covariance, G0 reproduction) and not by a fixture:
-  **GW parity unpinned at the fixture level**.
+* The GW self-energy (P0 -> W -> Sigma, with and without the "extrapolate"
+  q -> 0 correction, scalar and two-component) is pinned against the
+  reference's three GW fixtures (test/data/GW data.h5 and data_c.h5,
+  test/data/GW_X2C): the fixture's G_tau, replayed on transforms built for the
+  fixture's own IR tau points (gb200.grids.SampledGrid; the green-grids file
+  ``ir/1e4.h5`` itself is external), reproduces ``result/Sigma_tau`` within
+  the reference test's absolute 1e-6 (measured 8.9e-9, 2.8e-11, 1.2e-11) —
+  see tests/test_gw_golden.py.
+* The Dyson step follows the same reference code and is pinned by identities
+  (G0 reproduction, the chemical-potential search's electron count).
 
 Array conventions (row-major, as the reference):
   G, Sigma : [nts, ns, nk, nso, nso]            (mbpt_run.h:260-263)
@@ -80,6 +84,33 @@ class NoSymBZ:
     def kminus_table(self):
         """table[k, q] = k2_from_k1q(k, q)."""
         return np.array([[self.k2_from_k1q(k, q) for q in range(self.nk)] for k in range(self.nk)], dtype=np.int32)
+
+
+class PointsBZ(NoSymBZ):
+    """The k_q_map of a mesh given by the fractional coordinates of its points (an input file's
+    symmetry/k/mesh_scaled), in the file's own point order: k + q and k - q are looked up modulo
+    reciprocal lattice vectors (the same semantics as NoSymBZ)."""
+
+    def __init__(self, frac):
+        self.f = np.asarray(frac, dtype=np.float64).reshape(-1, 3)
+        self.nk = len(self.f)
+
+    def _lookup(self, v):
+        d = self.f - v
+        d = np.abs(d - np.round(d)).max(axis=1)
+        i = int(np.argmin(d))
+        if d[i] > 1e-6:
+            raise ValueError("k-point set is not closed under addition")
+        return i
+
+    def k1_from_k2q(self, k2, q):
+        return self._lookup(self.f[k2] + self.f[q])
+
+    def k2_from_k1q(self, k1, q):
+        return self._lookup(self.f[k1] - self.f[q])
+
+    def q_from_k1k2(self, k1, k2):
+        return self._lookup(self.f[k1] - self.f[k2])
 
 
 def pair_index(k1, k2):

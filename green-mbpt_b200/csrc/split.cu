@@ -23,8 +23,8 @@
 // Tensor-core kernel.  One CTA computes 128 real rows x BN complex columns for
 // all S diagonals (S * BN <= 512 TMEM columns).  Warp 0 streams 64-byte K blocks
 // of every slice plane with TMA (64-byte swizzle) through a multi-stage mbarrier
-// ring, warp 1 issues the tcgen05.mma instructions from one thread, and warps
-// 2-5 read the accumulators from TMEM (tcgen05.ld) and recombine in FP64.  Every
+// ring, warp 1 issues the tcgen05.mma instructions from one thread, and 16
+// epilogue warps read the accumulators from TMEM (tcgen05.ld) and recombine in FP64.  Every
 // wait is bounded; on timeout the kernel records an error and returns.
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -43,11 +43,14 @@ namespace {
 
 constexpr int KBLK = 64;          // bytes of K per pipeline stage (one 64B swizzle atom)
 constexpr int TILE_M = 128;       // real rows per CTA (64 complex rows)
-constexpr int EPI_CH = 32;        // result columns staged per epilogue step
-constexpr int EPI_LD = EPI_CH + 1; // staging row stride in complex values (one extra spreads the banks)
-constexpr int SMEM_BUDGET = 200 * 1024;
-constexpr int NWARPS = 10;        // producer, MMA, 8 epilogue warps
-constexpr int EPI_THREADS = 256;
+constexpr int SMEM_BUDGET = 216 * 1024;  // TMA ring + tables, under the 227 KB opt-in
+constexpr int EPI_WARPS = 16;     // four per TMEM sub-partition: enough warps in flight to hide
+                                  // the TMEM, FP64 and store latencies of the recombination
+constexpr int NWARPS = 2 + EPI_WARPS;  // producer, MMA, epilogue warps
+constexpr int EPI_THREADS = EPI_WARPS * 32;
+constexpr int EPI_CH = 32;                          // result columns per epilogue step
+constexpr int EPI_CG = EPI_CH / (EPI_WARPS / 4);  // columns of a step per epilogue warp
+static_assert(EPI_CG == 8, "epilogue column group: one tcgen05.ld of 8 columns");
 constexpr long long WAIT_LIMIT = 4000000000LL;  // clock64 cycles (~2 s)
 
 enum SplitErr { SERR_NONE = 0, SERR_TIMEOUT_PRODUCER = 1, SERR_TIMEOUT_MMA = 2, SERR_TIMEOUT_EPILOGUE = 3 };
@@ -126,13 +129,13 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&v)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr));
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, int32_t (&v)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr));
 }
+
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory"); }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
@@ -186,6 +189,7 @@ struct GemmParams {
   ZResult C;
   cplx alpha, beta;
   int alpha_pow2;  // alpha is real and a power of two (possibly negative)
+  int pair;        // the chunk is short enough that diagonal pairs (0,1), (2,3) fit int32 exactly
   int* err;
 };
 
@@ -487,6 +491,34 @@ __device__ __forceinline__ void store_result(const GemmParams& p, int64_t b0, in
   store_at(p, Cb + p.C.row(m) + p.C.col(n), re, im, ea, eb);
 }
 
+// Horner sum of the S diagonals of W accumulator columns, as combine_diagonals.  With `pair`
+// (host check: |q_d| bounded by the chunk length) q_d 128 + q_(d+1) is exact in int32 for the
+// pairs (0,1) and (2,3), and the Horner sum over the pairs equals the one over single diagonals,
+// since every partial sum below 2^53 is exact.
+template <int S, int W>
+__device__ __forceinline__ void combine_cols(const int32_t (&q)[S][1][W], bool pair, double (&v)[W]) {
+  if constexpr (S <= 5) {
+    if (pair) {
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        double a = int_to_double(q[0][0][j] * 128 + q[1][0][j]);
+        if constexpr (S >= 4) a = fma(a, 16384.0, int_to_double(q[2][0][j] * 128 + q[3][0][j]));
+        if constexpr (S == 3) a = fma(a, 128.0, int_to_double(q[2][0][j]));
+        if constexpr (S == 5) a = fma(a, 128.0, int_to_double(q[4][0][j]));
+        v[j] = a;
+      }
+      return;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+    double a = 0.0;
+#pragma unroll
+    for (int d = 0; d < S; ++d) a = fma(a, 128.0, int_to_double(q[d][0][j]));
+    v[j] = a;
+  }
+}
+
 // ----------------------------------------------------------------------------
 // tcgen05 core
 // ----------------------------------------------------------------------------
@@ -501,13 +533,18 @@ __host__ __device__ inline SmemLayout smem_layout(int S, int BN, int stages) {
   L.stage_bytes = S * (L.a_plane_bytes + L.b_plane_bytes);
   L.stages = stages;
   L.ring_bytes = stages * L.stage_bytes;
-  L.ctile_bytes = ((TILE_M / 2) * EPI_LD * 16 + 1023) / 1024 * 1024;
+  L.ctile_bytes = 0;  // the epilogue stores from registers (no staging tile)
   return L;
 }
 
-// bytes after the tile ring and the result tile: barriers, TMEM slot, flags, per-tile tables
+// one set of per-tile epilogue tables: row and column offsets of C, column factors, exponents
+__host__ __device__ inline int table_set_bytes(int BN) {
+  return ((TILE_M / 2) * 8 + BN * 16 + (TILE_M / 2 + BN) * 4 + 15) / 16 * 16;
+}
+
+// bytes after the tile ring: barriers, TMEM slot, flags, two sets of per-tile tables
 __host__ __device__ inline int misc_bytes(int stages, int BN) {
-  return (2 * stages + 4) * 8 + 16 + (TILE_M / 2 + BN) * 4 + (TILE_M / 2 + BN) * 8 + BN * 8 + 64;
+  return (2 * stages + 4) * 8 + 32 + 2 * table_set_bytes(BN) + 64;
 }
 
 struct TileCoord {
@@ -537,7 +574,7 @@ __device__ __forceinline__ TileCoord tile_coord(const GemmParams& p, int64_t t) 
 // Persistent tensor-core kernel: every CTA walks tiles blockIdx.x, +gridDim.x, ...
 //  warp 0       TMA producer (one thread), a ring of `stages` K blocks that runs across tiles
 //  warp 1       MMA issuer (one thread), `nbuf` TMEM accumulator sets of S * BN columns
-//  warps 2..5   epilogue: TMEM -> FP64 tile in shared memory -> coalesced global stores
+//  warps 2..    epilogue (EPI_WARPS): TMEM -> registers -> FP64 recombination -> stores to C
 // With nbuf = 2 the epilogue of one tile overlaps the MMAs of the next.
 template <int SS>
 __global__ void __launch_bounds__(NWARPS * 32, 1)
@@ -546,7 +583,6 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const SmemLayout L = smem_layout(p.S, p.BN, p.stages);
   uint8_t* tiles = smem;
-  cplx* ctile = reinterpret_cast<cplx*>(smem + L.ring_bytes);
   uint64_t* full_bar = reinterpret_cast<uint64_t*>(smem + L.ring_bytes + L.ctile_bytes);
   uint64_t* empty_bar = full_bar + L.stages;
   uint64_t* accf_bar = empty_bar + L.stages;   // [2]
@@ -554,12 +590,9 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
   uint8_t* misc = reinterpret_cast<uint8_t*>(acce_bar + 2);
   uint32_t* tmem_base_slot = reinterpret_cast<uint32_t*>(misc);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(misc + 4);
-  volatile int* epi_ok = reinterpret_cast<volatile int*>(misc + 8);
-  int32_t* sh_eA = reinterpret_cast<int32_t*>(misc + 16);
-  int32_t* sh_eB = sh_eA + TILE_M / 2;
-  int64_t* sh_rowC = reinterpret_cast<int64_t*>(misc + 16 + ((TILE_M / 2 + p.BN) * 4 + 7) / 8 * 8);
-  int64_t* sh_colC = sh_rowC + TILE_M / 2;
-  double* sh_csc = reinterpret_cast<double*>(sh_colC + p.BN);  // column factors 2^(eb - 7(S+1))
+  volatile int* epi_ok = reinterpret_cast<volatile int*>(misc + 8);  // [2], per tile parity
+  uint8_t* tables = misc + 32;                                          // [2] table sets
+  const int tsb = table_set_bytes(p.BN);
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   constexpr int S = SS;
@@ -576,10 +609,10 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&accf_bar[b], 1);
-      mbar_init(&acce_bar[b], 1);
+      mbar_init(&acce_bar[b], EPI_WARPS);  // every epilogue warp releases the set it has read
     }
     *abort_flag = 0;
-    *epi_ok = 1;
+    epi_ok[0] = epi_ok[1] = 1;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
@@ -662,18 +695,29 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
       }
     }
   } else {
-    // epilogue warps 2..9: TMEM sub-partition = warp % 4; the two warps of a sub-partition
-    // take alternate 16-column groups
+    // epilogue warps: TMEM sub-partition = warp % 4; the EPI_WARPS / 4 warps of a sub-partition
+    // take consecutive EPI_CG-column groups of each step.  Lanes 2j and 2j+1 hold the real and
+    // imaginary row of one complex result row; one shuffle gives each lane both parts of half of
+    // its columns, which it stores straight to C.  The tables of consecutive tiles alternate
+    // between two sets, so one named barrier per tile separates their writes from their reads.
     const int sp = warp % 4;
-    const int half = (warp - 2) / 4;
+    const int grp = (warp - 2) / 4;
     const int row = sp * 32 + lane;  // real row inside the tile
-    const int et = threadIdx.x - 64;  // 0..255
+    const int et = threadIdx.x - 64;  // 0..EPI_THREADS-1
+    const int mloc = row / 2;
+    const int r = row & 1;
+    constexpr int H = EPI_CG / 2;
     int64_t tcount = 0;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
       const TileCoord tc = tile_coord(p, t);
       const int buf = (int)(tcount % nbuf);
       const int64_t use = tcount / nbuf;
-      // per-tile tables (the previous tile's write-out finished at the last barrier)
+      uint8_t* tb = tables + (tcount & 1) * tsb;
+      int64_t* sh_rowC = reinterpret_cast<int64_t*>(tb);
+      int64_t* sh_colC = sh_rowC + TILE_M / 2;
+      double* sh_csc = reinterpret_cast<double*>(sh_colC + p.BN);  // column factors 2^(eb - 7(S+1))
+      int32_t* sh_eA = reinterpret_cast<int32_t*>(sh_csc + p.BN);
+      // (filled while the MMAs of this tile run)
       for (int i = et; i < TILE_M / 2 + p.BN; i += EPI_THREADS) {
         if (i < TILE_M / 2) {
           const int64_t m = tc.mrow0 / 2 + i;
@@ -681,9 +725,9 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
           sh_rowC[i] = m < p.M ? p.C.row(m) : 0;
         } else {
           const int64_t n = tc.ncol0 + (i - TILE_M / 2);
-          sh_eB[i - TILE_M / 2] = n < p.N ? p.eB[tc.rbB * p.eB_ld + n] : 0;
+          const int eb = n < p.N ? p.eB[tc.rbB * p.eB_ld + n] : 0;
           sh_colC[i - TILE_M / 2] = n < p.N ? p.C.col(n) : 0;
-          sh_csc[i - TILE_M / 2] = pow2(sh_eB[i - TILE_M / 2] - 7 * (S + 1));
+          sh_csc[i - TILE_M / 2] = pow2(eb - 7 * (S + 1));
         }
       }
       if (et == 0) {
@@ -692,86 +736,64 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
           atomicExch(p.err, SERR_TIMEOUT_EPILOGUE);
           *abort_flag = 1;
         }
-        *epi_ok = ok ? 1 : 0;
+        epi_ok[tcount & 1] = ok ? 1 : 0;
       }
       // every epilogue thread reaches every named barrier, on the error path too
-      asm volatile("bar.sync 1, 256;" ::: "memory");
-      if (!*epi_ok) break;
+      epi_bar();
+      if (!epi_ok[tcount & 1]) break;
       tc_fence_after();
-      const int mloc = row / 2;
-      const int r = row & 1;
       // a real alpha that is a power of two is folded into the row factor (exact, so the result
-      // equals the validation engine's alpha * value); the write-out is then a plain copy
+      // equals the validation engine's alpha * value); the store is then a plain copy
       const bool alpha_in_tile = p.alpha_pow2 != 0;
       const double rs = alpha_in_tile ? pow2(sh_eA[mloc]) * p.alpha.x : pow2(sh_eA[mloc]);
       // a warp whose 32 rows are all padding skips the accumulator reads
       const bool live = tc.mrow0 + sp * 32 < 2 * p.M;
       const uint32_t acc = tmem_base + (uint32_t)buf * acc_cols + ((uint32_t)(sp * 32) << 16);
       const int64_t mlim = p.M - tc.mrow0 / 2, nlim = p.N - tc.ncol0;
-      cplx* Cb = p.C.ptr + p.C.bat(tc.b0, tc.b1, tc.b2);
+      const bool mok = mloc < mlim;
+      cplx* Crow = p.C.ptr + p.C.bat(tc.b0, tc.b1, tc.b2) + sh_rowC[mloc];
       const bool has_beta = p.beta.x != 0.0 || p.beta.y != 0.0;
       for (int c0 = 0; c0 < p.BN; c0 += EPI_CH) {
         const int cw = min(EPI_CH, p.BN - c0);
-        const int cc = half * 16;
-        if (live && cc < cw) {
-          // TMEM -> FP64 complex chunk: real rows write .x, imaginary rows .y.  The diagonals are
-          // combined by Horner's rule in FP64 as in combine_diagonals (the first step from 0 is
-          // exact), then scaled by result_scale's two factors.
-          double accd[16];
+        const int cc = grp * EPI_CG;
+        const bool last = c0 + EPI_CH >= p.BN;
+        double v[EPI_CG];
+        const bool work = live && cc < cw;
+        if (work) {
+          // all S diagonals of the warp's 8 columns in one TMEM round trip
+          int32_t q[S][1][EPI_CG];
 #pragma unroll
-          for (int j = 0; j < 16; ++j) accd[j] = 0.0;
-          // up to six diagonals per TMEM round trip (all of them for S <= 6)
-          constexpr int DB = S <= 6 ? S : 4;
+          for (int d = 0; d < S; ++d) tmem_ld8(acc + (uint32_t)(d * p.BN + c0 + cc), q[d][0]);
+          tmem_wait_ld();
+          combine_cols<S, EPI_CG>(q, p.pair != 0, v);
+        }
+        if (last) {
+          // this warp's reads of the accumulator set are complete: release it to the MMA warp
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive_local(&acce_bar[buf]);
+        }
+        if (work) {
 #pragma unroll
-          for (int d0 = 0; d0 < S; d0 += DB) {
-            int32_t q[DB][16];
+          for (int j = 0; j < EPI_CG; ++j) v[j] *= rs * sh_csc[c0 + cc + j];
+          // the even lane keeps columns [0, H) of the group, the odd lane [H, 2H)
+          double other[H];
 #pragma unroll
-            for (int dd = 0; dd < DB; ++dd)
-              if (d0 + dd < S) tmem_ld16(acc + (uint32_t)((d0 + dd) * p.BN + c0 + cc), q[dd]);
-            tmem_wait_ld();
+          for (int i = 0; i < H; ++i) other[i] = __shfl_xor_sync(0xffffffffu, r ? v[i] : v[H + i], 1);
+          if (mok) {
 #pragma unroll
-            for (int dd = 0; dd < DB; ++dd) {
-              if (d0 + dd < S) {
-#pragma unroll
-                for (int j = 0; j < 16; ++j) accd[j] = fma(accd[j], 128.0, int_to_double(q[dd][j]));
+            for (int i = 0; i < H; ++i) {
+              const int col = c0 + cc + (r ? H + i : i);
+              if (col < nlim) {
+                cplx* d = Crow + sh_colC[col];
+                cplx val = r ? cmk(other[i], v[H + i]) : cmk(v[i], other[i]);
+                if (!alpha_in_tile) val = cmul(p.alpha, val);
+                if (has_beta) val = cadd(val, cmul(p.beta, *d));
+                *d = val;
               }
             }
           }
-#pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const double v = accd[j] * (rs * sh_csc[c0 + cc + j]);
-            reinterpret_cast<double*>(&ctile[mloc * EPI_LD + cc + j])[r] = v;
-          }
         }
-        const bool last = c0 + EPI_CH >= p.BN;
-        if (last) tc_fence_before();
-        asm volatile("bar.sync 1, 256;" ::: "memory");
-        if (last && et == 0) mbar_arrive_local(&acce_bar[buf]);  // this accumulator set may be reused
-        // coalesced write-out: consecutive threads walk the result index with unit stride
-        // (four elements per round, their loads ahead of their stores)
-        const int total = (TILE_M / 2) * cw;
-        for (int e0 = et; e0 < total; e0 += 4 * EPI_THREADS) {
-          cplx v[4];
-          cplx* d[4];
-          bool ok[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const int e = e0 + u * EPI_THREADS;
-            int ml, nl;
-            if (p.rows_fast) { ml = e % (TILE_M / 2); nl = e / (TILE_M / 2); } else { nl = e % cw; ml = e / cw; }
-            ok[u] = e < total && ml < mlim && c0 + nl < nlim;
-            d[u] = ok[u] ? Cb + sh_rowC[ml] + sh_colC[c0 + nl] : nullptr;
-            v[u] = ok[u] ? ctile[ml * EPI_LD + nl] : cmk(0.0, 0.0);
-          }
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            if (!ok[u]) continue;
-            cplx val = alpha_in_tile ? v[u] : cmul(p.alpha, v[u]);
-            if (has_beta) val = cadd(val, cmul(p.beta, *d[u]));
-            *d[u] = val;
-          }
-        }
-        asm volatile("bar.sync 1, 256;" ::: "memory");
       }
     }
   }
@@ -951,10 +973,11 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st, i
   const int S = slices > 0 ? slices : c.slices;
   require(S >= 2 && S <= 8, GB200_ERR_INVALID, "split: slices out of range");
   require(g0.K > 0, GB200_ERR_INVALID, "split: empty contraction");
-  // One TMEM accumulator set of up to 512 columns and the widest tile it allows: the cost per
-  // tile is largely fixed (tables, barriers, TMEM round trips), and halving the tile width to
-  // double-buffer the accumulators (so that the epilogue overlaps the next tile's MMAs) measured
-  // 20-27% slower for the short contractions on B200.
+  // One TMEM accumulator set of up to 512 columns and the widest tile it allows.  Measured on
+  // B200 for every launch shape of the GW chain, this is faster than two sets of half the width
+  // (the epilogue of one tile overlapping the next tile's MMAs), with one MMA per slice product
+  // or with one MMA of width (S - s) BN per A slice plane: narrower tiles double the per-tile
+  // epilogue work (tables, barrier, TMEM round trips) that dominates the short contractions.
   const int nbuf = 1;
   const int BN = std::min<int>(max_bn(S, 512 / nbuf), (int)rup(g0.N, 16));
   // largest K chunk for which no INT32 diagonal can overflow: S * 2K * 127^2 < 2^31
@@ -1010,6 +1033,14 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st, i
     {
       int aexp = 0;
       p.alpha_pow2 = (g0.alpha.y == 0.0 && g0.alpha.x != 0.0 && std::fabs(std::frexp(g0.alpha.x, &aexp)) == 0.5) ? 1 : 0;
+    }
+    {
+      // |q_d| <= (d + 1) * 2Kc * 64^2 (d + 1 digit pairs per diagonal, balanced digits |q| <= 64):
+      // pair (d, d + 1) is exact in int32 when 128 max|q_d| + max|q_(d+1)| < 2^31
+      bool ok = S <= 5;
+      for (int d = 0; ok && d + 1 < S && d <= 2; d += 2)
+        ok = 2.0 * (double)Kc * 4096.0 * (128.0 * (d + 1) + (d + 2)) < 2147483648.0;
+      p.pair = ok ? 1 : 0;
     }
     p.rows_fast = std::abs(g0.C.row.s_in) < std::abs(g0.C.col.s_in) ? 1 : 0;
     const int64_t nbatch = g0.nb0 * g0.nb1 * g0.nb2;

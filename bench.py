@@ -201,14 +201,19 @@ def setup_context(cfg, seed, slices, device, ws, rank, contraction_slices=None, 
     kp, km = solvers.kq_maps(s.mesh)
     ctx.set_kq_maps(kp, km)
     ctx.set_grid(g.Tnt_f, g.Ttn_f, g.Tnt_b, g.Ttn_b, g.wsample_f)
-    synth.upload_device_integrals(ctx, s.nk, s.NQ, s.nao, seed=seed, device=device)
+    if ws > 1:
+        # q-sharded: this rank keeps only the integral pairs of its q range
+        q0, q1 = shard.q_shard(s.nk, ws, rank)
+        synth.upload_device_integral_pairs(ctx, s.nk, s.NQ, s.nao, shard.pairs_for_q_range(kp, q0, q1), seed=seed,
+                                           device=device)
+        ctx.set_q_range(q0, q1)
+    else:
+        synth.upload_device_integrals(ctx, s.nk, s.NQ, s.nao, seed=seed, device=device)
     ctx.set_hamiltonian(s.F, s.S)
     ctx.set_precision(lib.PREC_SPLIT, slices)
     ctx.set_split_engine(engine)
     if contraction_slices:
         ctx.set_contraction_slices(contraction_slices)
-    if ws > 1:
-        ctx.set_q_range(*shard.q_shard(s.nk, ws, rank))
     return s, ctx
 
 
@@ -250,10 +255,12 @@ def run_ours(args):
             state["mu"], state["E"] = ctx.iteration_device(G.data_ptr(), S1.data_ptr(), St.data_ptr(), mad, nel, tol,
                                                            state["mu"], stream=sptr)
             return
-        # q-sharded GW: partial self-energies are summed before the Dyson step
+        # q-sharded GW and HF exchange (each rank holds the integral pairs of its q range): the
+        # partial Fock matrices and self-energies are summed before the Dyson step
         dm.copy_(G[-1] * (-1.0 if s.ns == 2 else -2.0))
         ctx.hf_fock_device(dm.data_ptr(), Sdev.data_ptr(), mad, S1.data_ptr(), stream=sptr)
         ctx.gw_sigma_device(G.data_ptr(), St.data_ptr(), stream=sptr)
+        shard.reduce_partial_sigma(S1, dist)
         shard.reduce_partial_sigma(St, dist)
         state["mu"] = ctx.dyson_solve_device(S1.data_ptr(), St.data_ptr(), nel, tol, state["mu"], G.data_ptr(),
                                              stream=sptr)

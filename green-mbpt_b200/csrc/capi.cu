@@ -65,6 +65,26 @@ __global__ void scatter_pairs_kernel(const cplx* half_chunk, int64_t p0, int64_t
   }
 }
 
+// The same for an explicit list of stored pairs: pair l of the chunk goes to block slot[2l] as it
+// is and, unless it is a diagonal pair (slot[2l+1] < 0), to block slot[2l+1] as the per-Q
+// conjugate transpose.
+__global__ void scatter_pair_slots_kernel(const cplx* chunk, int64_t cnt, const int64_t* slot, cplx* V, int NQ,
+                                          int nao) {
+  const int64_t m2 = (int64_t)nao * nao;
+  const int64_t pe = (int64_t)NQ * m2;
+  const int64_t total = cnt * pe;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t lp = e / pe;
+    const int64_t r = e - lp * pe;
+    const int64_t Q = r / m2;
+    const int ij = (int)(r - Q * m2);
+    const int i = ij / nao, j = ij % nao;
+    const cplx v = chunk[e];
+    V[slot[2 * lp] * pe + r] = v;
+    if (slot[2 * lp + 1] >= 0) V[slot[2 * lp + 1] * pe + Q * m2 + (int64_t)j * nao + i] = cconj(v);
+  }
+}
+
 void upload_integrals(Context& c, DevArray<cplx>& dst, const double* V_half, int64_t npairs, bool on_device,
                       cudaStream_t st) {
   const int nk = c.d.nk;
@@ -227,7 +247,9 @@ int gb200_set_integrals(gb200_context* ctx, int which, const double* V_half, int
   return guarded(ctx, [&](Context& c) {
     require(V_half != nullptr, GB200_ERR_INVALID, "set_integrals: null pointer");
     if (which == GB200_INTEGRALS_GW) {
+      c.v_slot.clear();
       upload_integrals(c, c.V, V_half, npairs, false, c.stream);
+      if (c.have_kq) build_tables(c);
       c.have_V = true;
     } else if (which == GB200_INTEGRALS_HF) {
       upload_integrals(c, c.Vhf, V_half, npairs, false, c.stream);
@@ -429,6 +451,9 @@ int gb200_iteration_device(gb200_context* ctx, double* G_dev, double* Sigma1_dev
                            void* stream) {
   return guarded(ctx, [&](Context& c) {
     require(G_dev && Sigma1_dev && Sigma_dev && mu_inout, GB200_ERR_INVALID, "iteration: null pointer");
+    require(!c.v_subset(), GB200_ERR_STATE,
+            "iteration: the GW integrals hold a pair subset (partial self-energy): reduce across ranks and call "
+            "the Dyson step separately");
     cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
     const gb200_dims& d = c.d;
     cplx* G = reinterpret_cast<cplx*>(G_dev);
@@ -476,6 +501,10 @@ int gb200_set_integrals_device(gb200_context* ctx, int which, const double* V_de
     int64_t& done = which == GB200_INTEGRALS_GW ? c.pairs_set_gw : c.pairs_set_hf;
     const int64_t pe = c.pair_elems();
     if (pair_begin == 0) done = 0;
+    if (which == GB200_INTEGRALS_GW && c.v_subset()) {
+      c.v_slot.clear();  // back to the full pair set
+      if (c.have_kq) build_tables(c);
+    }
     dst.alloc((size_t)nk * nk * pe);
     scatter_pairs_kernel<<<148 * 16, 256, 0, st>>>(reinterpret_cast<const cplx*>(V_dev), pair_begin, pair_count, dst.p,
                                                    nk, c.d.NQ, c.d.nao);
@@ -487,6 +516,57 @@ int gb200_set_integrals_device(gb200_context* ctx, int which, const double* V_de
     } else {
       c.have_Vhf = done >= npairs;
     }
+  });
+}
+
+int gb200_set_integrals_pairs(gb200_context* ctx, const double* V_pairs, const int64_t* pair_ids, int64_t count,
+                              int on_device, void* stream) {
+  return guarded(ctx, [&](Context& c) {
+    require(V_pairs != nullptr && pair_ids != nullptr && count > 0, GB200_ERR_INVALID,
+            "set_integrals_pairs: null pointer or empty pair list");
+    const int nk = c.d.nk;
+    const int64_t npairs = (int64_t)nk * (nk + 1) / 2, pe = c.pair_elems();
+    std::vector<int64_t> slot_of((size_t)nk * nk, -1), slots((size_t)2 * count);
+    int64_t nblk = 0;
+    for (int64_t l = 0; l < count; ++l) {
+      const int64_t p = pair_ids[l];
+      require(p >= 0 && p < npairs && (l == 0 || p > pair_ids[l - 1]), GB200_ERR_INVALID,
+              "set_integrals_pairs: pair indices must increase strictly within [0, nk(nk+1)/2)");
+      int64_t k1 = (int64_t)((std::sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
+      while (k1 * (k1 + 1) / 2 > p) --k1;
+      while ((k1 + 1) * (k1 + 2) / 2 <= p) ++k1;
+      const int64_t k2 = p - k1 * (k1 + 1) / 2;
+      slots[2 * l] = slot_of[(size_t)(k1 * nk + k2)] = nblk++;
+      slots[2 * l + 1] = -1;
+      if (k1 != k2) slots[2 * l + 1] = slot_of[(size_t)(k2 * nk + k1)] = nblk++;
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : c.stream;
+    c.V.alloc((size_t)nblk * pe);
+    DevArray<int64_t> dslots;
+    dslots.upload(slots.data(), slots.size(), st);
+    const cplx* src = reinterpret_cast<const cplx*>(V_pairs);
+    if (on_device) {
+      scatter_pair_slots_kernel<<<148 * 16, 256, 0, st>>>(src, count, dslots.p, c.V.p, c.d.NQ, c.d.nao);
+      GB_CHECK_LAUNCH();
+    } else {
+      // stream the host blocks through a bounded staging buffer
+      const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(count, (int64_t)(1e9 / (pe * sizeof(cplx)))));
+      DevArray<cplx> stage;
+      stage.alloc((size_t)chunk * pe);
+      for (int64_t l0 = 0; l0 < count; l0 += chunk) {
+        const int64_t cnt = std::min(chunk, count - l0);
+        GB_CUDA(cudaMemcpyAsync(stage.p, src + l0 * pe, (size_t)cnt * pe * sizeof(cplx), cudaMemcpyHostToDevice, st));
+        scatter_pair_slots_kernel<<<148 * 16, 256, 0, st>>>(stage.p, cnt, dslots.p + 2 * l0, c.V.p, c.d.NQ, c.d.nao);
+        GB_CHECK_LAUNCH();
+        GB_CUDA(cudaStreamSynchronize(st));
+      }
+    }
+    GB_CUDA(cudaStreamSynchronize(st));
+    c.v_slot.swap(slot_of);
+    c.pairs_set_gw = count;
+    if (c.have_kq) build_tables(c);
+    build_subset_tables(c);
+    c.have_V = true;
   });
 }
 

@@ -105,14 +105,17 @@ struct Context {
   std::vector<double> q_abs;
   double q0_madelung = 0.0;
 
-  // integrals, all ordered pairs [nk][nk][NQ][nao][nao]
+  // integrals, all ordered pairs [nk][nk][NQ][nao][nao]; the GW set may instead hold a subset
+  // (q-sharded storage): then v_slot[k1 * nk + k2] is the block of (k1, k2) in V, -1 where this
+  // context does not hold it
   DevArray<cplx> V, Vhf;
+  std::vector<int64_t> v_slot;
   // Dyson inputs [ns][nk][nso][nso]
   DevArray<cplx> H, S;
 
   // per-q offset tables (device): [nq][nk] or [nq][nk*ns]
   DevArray<int64_t> tab_pair_plus, tab_pair_minus, tab_g_plus, tab_g_minus, tab_pair_plus_ns;
-  DevArray<int64_t> tab_pair_diag_ns;  // HF: pair (k,k) offset for index k*ns+s
+  DevArray<int64_t> tab_v_diag;  // pair subset: offset of block (k, k) in V per k (0 where not held)
 
   Scratch scratch;
   float timings[4] = {0, 0, 0, 0};
@@ -128,6 +131,12 @@ struct Context {
   // stage boundaries of the GW q loop (4 per q-point), read once after the loop
   std::vector<cudaEvent_t> qev;
 
+  bool v_subset() const { return !v_slot.empty(); }
+  // block index of the ordered pair (k1, k2) in V, -1 if it is not held
+  int64_t v_block(int k1, int k2) const {
+    const int64_t i = (int64_t)k1 * d.nk + k2;
+    return v_slot.empty() ? i : v_slot[(size_t)i];
+  }
   int64_t nao() const { return d.nao; }
   int64_t pair_elems() const { return (int64_t)d.NQ * d.nao * d.nao; }
   // two-component (X2C) input: nso = 2 nao, the GW contractions run over the 4 spin blocks
@@ -139,7 +148,9 @@ struct Context {
 
 // stages implemented in the .cu files
 void build_tables(Context& c);
-void build_hf_tables(Context& c);
+void build_subset_tables(Context& c);
+// GB200_ERR_STATE unless V holds every pair the q-points [q0, q1) read: (k, k+q) and (k, k-q)
+void require_q_pairs(const Context& c, int q0, int q1);
 void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st);
 // Gb = d/dG of Re sum conj(Sb) Sigma(G, V) (FP64; no two-component input, no q -> 0 correction);
 // with Vb non-null also d/dV on the full pair set [nk][nk][NQ][nao][nao] (zeroed here)

@@ -133,8 +133,10 @@ void build_tables(Context& c) {
     for (int k = 0; k < nk; ++k) {
       int kp = c.kplus[(size_t)k * nk + q];
       int km = c.kminus[(size_t)k * nk + q];
-      pp[(size_t)q * nk + k] = ((int64_t)k * nk + kp) * pe;   // V(k, k+q)
-      pm[(size_t)q * nk + k] = ((int64_t)k * nk + km) * pe;   // V(k, k-q)
+      // V(k, k+q) and V(k, k-q); a block this context does not hold gets offset 0 (the q-points
+      // that would read it are refused by require_q_pairs)
+      pp[(size_t)q * nk + k] = std::max<int64_t>(0, c.v_block(k, kp)) * pe;
+      pm[(size_t)q * nk + k] = std::max<int64_t>(0, c.v_block(k, km)) * pe;
       gp[(size_t)q * nk + k] = (int64_t)kp * ge;              // G(., ., k+q)
       gm[(size_t)q * nk + k] = (int64_t)km * ge;              // G(., ., k-q)
       for (int s = 0; s < ns; ++s) ppns[((size_t)q * nk + k) * ns + s] = pp[(size_t)q * nk + k];
@@ -147,13 +149,24 @@ void build_tables(Context& c) {
   GB_CUDA(cudaStreamSynchronize(c.stream));
 }
 
-void build_hf_tables(Context& c) {
-  const int nk = c.d.nk, ns = c.d.ns;
+void require_q_pairs(const Context& c, int q0, int q1) {
+  if (!c.v_subset()) return;
+  const int nk = c.d.nk;
+  for (int q = q0; q < q1; ++q)
+    for (int k = 0; k < nk; ++k) {
+      const int kp = c.kplus[(size_t)k * nk + q], km = c.kminus[(size_t)k * nk + q];
+      require(c.v_block(k, kp) >= 0 && c.v_block(k, km) >= 0, GB200_ERR_STATE,
+              "the GW integrals hold a pair subset without V(k, k+-q) for q-point " + std::to_string(q) +
+                  " (k = " + std::to_string(k) + "): set the q range the subset was chosen for");
+    }
+}
+
+void build_subset_tables(Context& c) {
+  const int nk = c.d.nk;
   const int64_t pe = c.pair_elems();
-  std::vector<int64_t> dns((size_t)nk * ns);
-  for (int k = 0; k < nk; ++k)
-    for (int s = 0; s < ns; ++s) dns[(size_t)k * ns + s] = ((int64_t)k * nk + k) * pe;  // pair (k,k)
-  c.tab_pair_diag_ns.upload(dns.data(), dns.size(), c.stream);
+  std::vector<int64_t> dg(nk);
+  for (int k = 0; k < nk; ++k) dg[k] = std::max<int64_t>(0, c.v_block(k, k)) * pe;  // block (k, k)
+  c.tab_v_diag.upload(dg.data(), dg.size(), c.stream);
   GB_CUDA(cudaStreamSynchronize(c.stream));
 }
 
@@ -333,6 +346,7 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
   // the partial Sigma is already divided by nk, so shards sum to the full self-energy
   const int q0 = std::max(0, c.q_begin);
   const int q1 = c.q_end < 0 ? nk : std::min(nk, c.q_end);
+  require_q_pairs(c, q0, q1);
   // stage timings: events recorded on the stream and read after the loop, so the host never
   // waits inside it
   const size_t nev = (size_t)std::max(0, q1 - q0) * 4;

@@ -116,6 +116,7 @@ void gw_sigma_vjp(Context& c, const cplx* G, const cplx* Sb, cplx* Gb, cplx* Vb,
   require(c.have_kq && c.have_grid && c.have_V, GB200_ERR_STATE, "gw_sigma_vjp: k/q maps, grid and integrals must be set");
   require(!c.x2c(), GB200_ERR_INVALID, "gw_sigma_vjp: two-component input is not supported by the adjoint");
   require(!c.q0_on, GB200_ERR_INVALID, "gw_sigma_vjp: the q->0 correction is not supported by the adjoint");
+  require(!c.v_subset(), GB200_ERR_INVALID, "gw_sigma_vjp: needs all integral pairs (the adjoint runs every q-point)");
   const int nk = d.nk, ns = d.ns, nts = d.nts, nth = nts / 2, NQ = d.NQ, nw_b = d.nw_b;
   const int64_t nao = d.nao, nao2 = nao * nao, pe = c.pair_elems(), nq2 = (int64_t)NQ * NQ;
   const int64_t ge = nao2, g_s = (int64_t)nk * ge, g_t = (int64_t)ns * g_s;

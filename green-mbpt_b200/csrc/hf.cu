@@ -50,6 +50,12 @@ __global__ void diag_pair_table_kernel(int64_t* tab, int nk, int nb, int64_t pe)
   if (i < nk * nb) tab[i] = ((int64_t)(i / nb) * nk + i / nb) * pe;
 }
 
+// the same from the per-k offsets of the diagonal blocks of a pair subset
+__global__ void diag_slot_table_kernel(int64_t* tab, const int64_t* vdiag, int nk, int nb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nk * nb) tab[i] = vdiag[i / nb];
+}
+
 // two-component dm [nk][2n][2n] -> blocks aa, bb, ab [3][nk][n][n]; S -> S_aa [nk][n][n]
 __global__ void x2c_split_kernel(const cplx* dm, const cplx* S, cplx* blk, cplx* Saa, int nk, int n) {
   const int64_t n2 = (int64_t)n * n, total = (int64_t)nk * n2;
@@ -95,14 +101,27 @@ ZOperand dense(const cplx* p, int64_t ld) {
 //   Madelung F[b] -= mad_coef * S[b] dm[b] S[b], S[b][k] at S + b * s_block_stride + k * nao^2.
 // The scalar kernel is nsp = ndir = ns, pref = mad_coef = 0.5 (ns = 1) or 1; the two-component
 // kernel is the blocks (aa, bb, ab), ndir = 2, pref = mad_coef = 1.
+// `sub` (the GW integrals hold the pair subset of the context's q range, used when no separate HF
+// integrals are set): the exchange sums k' = k + q over that q range only, and the direct and
+// Madelung terms belong to the context whose range holds q = 0, so the partial Fock matrices of
+// ranks that split the q-points add up to the full one.
 static void hf_core(Context& c, const cplx* V, const cplx* dm, int nsp, int ndir, double pref, double madelung,
                     double mad_coef, const cplx* S, int64_t s_block_stride, cplx* F, cudaStream_t st) {
   const gb200_dims& d = c.d;
   const int nk = d.nk, NQ = d.NQ;
   const int64_t nao = d.nao, nao2 = nao * nao, pe = c.pair_elems();
   GB_CUDA(cudaMemsetAsync(F, 0, (size_t)nsp * nk * nao2 * sizeof(cplx), st));
+  const bool sub = V == c.V.get() && c.v_subset();
+  int q0 = 0, q1 = nk;
+  if (sub) {
+    require(c.have_kq, GB200_ERR_STATE, "hf_fock: a pair subset of the integrals needs the k/q maps");
+    q0 = std::max(0, c.q_begin);
+    q1 = c.q_end < 0 ? nk : std::min(nk, c.q_end);
+    require_q_pairs(c, q0, q1);
+  }
+  const bool own_q0 = !sub || (q0 == 0 && q1 > 0);
   // ---- direct (Hartree) term ----
-  if (ndir > 0) {
+  if (ndir > 0 && own_q0) {
     cplx* dmT = (cplx*)c.scratch.get(SL_HF_DMT, (size_t)ndir * nk * nao2 * sizeof(cplx));
     cplx* u = (cplx*)c.scratch.get(SL_HF_U, (size_t)NQ * sizeof(cplx));
     int64_t* tab = (int64_t*)c.scratch.get(SL_HF_TAB, (size_t)nk * ndir * sizeof(int64_t));
@@ -111,7 +130,8 @@ static void hf_core(Context& c, const cplx* V, const cplx* dm, int nsp, int ndir
       unsigned g = (unsigned)std::min<int64_t>((total + 255) / 256, 148 * 16);
       dm_transpose_kernel<<<std::max(1u, g), 256, 0, st>>>(dm, dmT, ndir, nk, (int)nao);
       GB_CHECK_LAUNCH();
-      diag_pair_table_kernel<<<(unsigned)((nk * ndir + 255) / 256), 256, 0, st>>>(tab, nk, ndir, pe);
+      if (sub) diag_slot_table_kernel<<<(unsigned)((nk * ndir + 255) / 256), 256, 0, st>>>(tab, c.tab_v_diag.get(), nk, ndir);
+      else diag_pair_table_kernel<<<(unsigned)((nk * ndir + 255) / 256), 256, 0, st>>>(tab, nk, ndir, pe);
       GB_CHECK_LAUNCH();
     }
     ZGemm g;  // u[Q] = (1/nk) sum_{(k,b),(a,a')} V(k,k)[Q][a][a'] dmT[(k,b)][a][a']
@@ -126,50 +146,80 @@ static void hf_core(Context& c, const cplx* V, const cplx* dm, int nsp, int ndir
     h.nb0 = nk; h.nb2 = ndir;
     h.A.ptr = u; h.A.row = lin(0); h.A.col = lin(1);
     h.B.ptr = V; h.B.row = lin(nao2); h.B.col = lin(1);
-    h.B.bat.s0 = ((int64_t)nk + 1) * pe;  // pair (k,k) of the full [nk][nk] storage
+    if (sub) h.B.bat.tab0 = c.tab_v_diag.get();  // block (k,k) of the subset
+    else h.B.bat.s0 = ((int64_t)nk + 1) * pe;     // pair (k,k) of the full [nk][nk] storage
     h.C.ptr = F; h.C.row = lin(0); h.C.col = lin(1);
     h.C.bat.s0 = nao2; h.C.bat.s2 = (int64_t)nk * nao2;
     h.beta = cmk(1.0, 0.0);
     zgemm_fp64(h, st);
+  }
+  // ---- exchange term over the q range of a pair subset: per q, all k at once ----
+  if (sub) {
+    cplx* Y = (cplx*)c.scratch.get(SL_HF_Y, (size_t)nk * nsp * pe * sizeof(cplx));
+    for (int q = q0; q < q1; ++q) {
+      const int64_t* tVp = c.tab_pair_plus.get() + (int64_t)q * nk;  // V(k, k+q)
+      const int64_t* tDp = c.tab_g_plus.get() + (int64_t)q * nk;     // block k+q of dm
+      ZGemm y;  // Y[k][b][(Q,i)][a] = sum_a' V(k,k+q)[(Q,i)][a'] dm[b][k+q][a'][a]
+      y.M = (int64_t)NQ * nao; y.N = nao; y.K = nao;
+      y.nb0 = nk; y.nb1 = nsp;
+      y.A = dense(V, nao); y.A.bat.tab0 = tVp;
+      y.B = dense(dm, nao); y.B.bat.tab0 = tDp; y.B.bat.s1 = (int64_t)nk * nao2;
+      y.C.ptr = Y; y.C.row = lin(nao); y.C.col = lin(1);
+      y.C.bat.s0 = (int64_t)nsp * pe; y.C.bat.s1 = pe;
+      zgemm_fp64(y, st);
+      ZGemm x;  // F[b][k][i][j] -= (pref/nk) sum_{Q,a} Y[k][b][Q][i][a] conj(V(k,k+q)[Q][j][a])
+      x.M = nao; x.N = nao; x.K = (int64_t)NQ * nao;
+      x.nb0 = nk; x.nb1 = nsp;
+      x.A.ptr = Y; x.A.row = lin(nao); x.A.col = two(nao, 1, nao2);
+      x.A.bat.s0 = (int64_t)nsp * pe; x.A.bat.s1 = pe;
+      x.B.ptr = V; x.B.row = two(nao, 1, nao2); x.B.col = lin(nao); x.B.conj = true;
+      x.B.bat.tab0 = tVp;
+      x.C.ptr = F; x.C.row = lin(nao); x.C.col = lin(1);
+      x.C.bat.s0 = nao2; x.C.bat.s1 = (int64_t)nk * nao2;
+      x.alpha = cmk(-pref / nk, 0.0); x.beta = cmk(1.0, 0.0);
+      zgemm_fp64(x, st);
+    }
   }
   // ---- exchange term, blocked over k ----
   // Per k the exchange is an nao x nao result contracted over K = (k', Q, a), i.e. nk*NQ*nao
   // terms.  One batch of the second contraction per (k, b, k') keeps the GPU busy (a single
   // batch per k would leave most SMs idle); the per-k' partial results are then summed in k'
   // order by exchange_reduce_kernel, so the result is deterministic.
-  const int64_t per_k = (int64_t)nsp * nk * pe;
-  const double budget = c.budget_or(8e9, 0.5);
-  int kb = (int)std::max(1.0, std::floor(budget / ((double)per_k * sizeof(cplx))));
-  kb = std::min(kb, nk);
-  cplx* Y = (cplx*)c.scratch.get(SL_HF_Y, (size_t)kb * per_k * sizeof(cplx));
-  cplx* P = (cplx*)c.scratch.get(SL_TMP, (size_t)kb * nsp * nk * nao2 * sizeof(cplx));
-  for (int k0 = 0; k0 < nk; k0 += kb) {
-    const int kbk = std::min(kb, nk - k0);
-    ZGemm y;  // Y[kk][b][k'][(Q,i)][a] = sum_a' V(k,k')[(Q,i)][a'] dm[b][k'][a'][a]
-    y.M = (int64_t)NQ * nao; y.N = nao; y.K = nao;
-    y.nb0 = kbk; y.nb1 = nsp; y.nb2 = nk;
-    y.A = dense(V + (int64_t)k0 * nk * pe, nao);
-    y.A.bat.s0 = (int64_t)nk * pe; y.A.bat.s2 = pe;
-    y.B = dense(dm, nao); y.B.bat.s1 = (int64_t)nk * nao2; y.B.bat.s2 = nao2;
-    y.C.ptr = Y; y.C.row = lin(nao); y.C.col = lin(1);
-    y.C.bat.s0 = per_k; y.C.bat.s1 = (int64_t)nk * pe; y.C.bat.s2 = pe;
-    zgemm_fp64(y, st);
-    ZGemm x;  // P[kk][b][k'][i][j] = sum_{Q,a} Y[kk][b][k'][Q][i][a] conj(V(k,k')[Q][j][a])
-    x.M = nao; x.N = nao; x.K = (int64_t)NQ * nao;
-    x.nb0 = kbk; x.nb1 = nsp; x.nb2 = nk;
-    x.A.ptr = Y; x.A.row = lin(nao); x.A.col = two(nao, 1, nao2);
-    x.A.bat.s0 = per_k; x.A.bat.s1 = (int64_t)nk * pe; x.A.bat.s2 = pe;
-    x.B.ptr = V + (int64_t)k0 * nk * pe; x.B.row = two(nao, 1, nao2); x.B.col = lin(nao); x.B.conj = true;
-    x.B.bat.s0 = (int64_t)nk * pe; x.B.bat.s2 = pe;
-    x.C.ptr = P; x.C.row = lin(nao); x.C.col = lin(1);
-    x.C.bat.s0 = (int64_t)nsp * nk * nao2; x.C.bat.s1 = (int64_t)nk * nao2; x.C.bat.s2 = nao2;
-    zgemm_fp64(x, st);
-    const int64_t nout = (int64_t)kbk * nsp * nao2;
-    exchange_reduce_kernel<<<(unsigned)((nout + 255) / 256), 256, 0, st>>>(P, F, kbk, nsp, nk, k0, nao2, -pref / nk);
-    GB_CHECK_LAUNCH();
+  if (!sub) {
+    const int64_t per_k = (int64_t)nsp * nk * pe;
+    const double budget = c.budget_or(8e9, 0.5);
+    int kb = (int)std::max(1.0, std::floor(budget / ((double)per_k * sizeof(cplx))));
+    kb = std::min(kb, nk);
+    cplx* Y = (cplx*)c.scratch.get(SL_HF_Y, (size_t)kb * per_k * sizeof(cplx));
+    cplx* P = (cplx*)c.scratch.get(SL_TMP, (size_t)kb * nsp * nk * nao2 * sizeof(cplx));
+    for (int k0 = 0; k0 < nk; k0 += kb) {
+      const int kbk = std::min(kb, nk - k0);
+      ZGemm y;  // Y[kk][b][k'][(Q,i)][a] = sum_a' V(k,k')[(Q,i)][a'] dm[b][k'][a'][a]
+      y.M = (int64_t)NQ * nao; y.N = nao; y.K = nao;
+      y.nb0 = kbk; y.nb1 = nsp; y.nb2 = nk;
+      y.A = dense(V + (int64_t)k0 * nk * pe, nao);
+      y.A.bat.s0 = (int64_t)nk * pe; y.A.bat.s2 = pe;
+      y.B = dense(dm, nao); y.B.bat.s1 = (int64_t)nk * nao2; y.B.bat.s2 = nao2;
+      y.C.ptr = Y; y.C.row = lin(nao); y.C.col = lin(1);
+      y.C.bat.s0 = per_k; y.C.bat.s1 = (int64_t)nk * pe; y.C.bat.s2 = pe;
+      zgemm_fp64(y, st);
+      ZGemm x;  // P[kk][b][k'][i][j] = sum_{Q,a} Y[kk][b][k'][Q][i][a] conj(V(k,k')[Q][j][a])
+      x.M = nao; x.N = nao; x.K = (int64_t)NQ * nao;
+      x.nb0 = kbk; x.nb1 = nsp; x.nb2 = nk;
+      x.A.ptr = Y; x.A.row = lin(nao); x.A.col = two(nao, 1, nao2);
+      x.A.bat.s0 = per_k; x.A.bat.s1 = (int64_t)nk * pe; x.A.bat.s2 = pe;
+      x.B.ptr = V + (int64_t)k0 * nk * pe; x.B.row = two(nao, 1, nao2); x.B.col = lin(nao); x.B.conj = true;
+      x.B.bat.s0 = (int64_t)nk * pe; x.B.bat.s2 = pe;
+      x.C.ptr = P; x.C.row = lin(nao); x.C.col = lin(1);
+      x.C.bat.s0 = (int64_t)nsp * nk * nao2; x.C.bat.s1 = (int64_t)nk * nao2; x.C.bat.s2 = nao2;
+      zgemm_fp64(x, st);
+      const int64_t nout = (int64_t)kbk * nsp * nao2;
+      exchange_reduce_kernel<<<(unsigned)((nout + 255) / 256), 256, 0, st>>>(P, F, kbk, nsp, nk, k0, nao2, -pref / nk);
+      GB_CHECK_LAUNCH();
+    }
   }
   // ---- Madelung / Ewald term ----
-  if (madelung != 0.0) {
+  if (madelung != 0.0 && own_q0) {
     cplx* T = (cplx*)c.scratch.get(SL_TMP, (size_t)nsp * nk * nao2 * sizeof(cplx));
     ZGemm a;  // T = S dm
     a.M = nao; a.N = nao; a.K = nao; a.nb1 = nsp; a.nb2 = nk;

@@ -61,7 +61,7 @@ EXPORTED = [
     "gb200_iteration_device", "gb200_last_timings", "gb200_set_split_engine", "gb200_set_integrals_device",
     "gb200_set_q_range", "gb200_dyson_solve_device", "gb200_energy_device", "gb200_stats_enable", "gb200_stats_read",
     "gb200_hf_fock_noalloc", "gb200_set_q0_correction", "gb200_gw_sigma_vjp", "gb200_gw_sigma_vjp_device",
-    "gb200_set_contraction_slices", "gb200_set_memory_budget",
+    "gb200_set_contraction_slices", "gb200_set_memory_budget", "gb200_set_integrals_pairs",
 ]
 
 
@@ -120,6 +120,7 @@ def load(path: str | None = None):
     L.gb200_stats_read.argtypes = [vp, ll, ll, dp, dp]
     L.gb200_hf_fock_noalloc.argtypes = [ctypes.POINTER(Dims), vp, vp, vp, ctypes.c_double, vp, vp]
     L.gb200_set_q0_correction.argtypes = [vp, vp, vp, ctypes.c_double]
+    L.gb200_set_integrals_pairs.argtypes = [vp, vp, vp, ctypes.c_int64, ip, vp]
     _lib = L
     return L
 
@@ -300,6 +301,20 @@ class Context:
         """Deliver stored pairs [pair_begin, pair_begin + pair_count) from device memory."""
         self._check(self._L.gb200_set_integrals_device(self._h, which, ctypes.c_void_p(V_ptr), pair_begin, pair_count,
                                                        ctypes.c_void_p(stream)))
+
+    def set_integrals_pairs(self, V_pairs, pair_ids, stream: int = 0):
+        """q-sharded GW integrals: the stored pairs `pair_ids` (increasing half-storage indices,
+        gb200.shard.pairs_for_q_range) with their blocks V_pairs [len, NQ, nao, nao]: a host
+        array, or the device address of such an array (an int)."""
+        ids = np.ascontiguousarray(pair_ids, dtype=np.int64)
+        if isinstance(V_pairs, int):
+            self._check(self._L.gb200_set_integrals_pairs(self._h, ctypes.c_void_p(V_pairs), _ptr(ids), len(ids), 1,
+                                                          ctypes.c_void_p(stream)))
+            return
+        V = _c128(V_pairs)
+        if V.shape[0] != len(ids):
+            raise ValueError("set_integrals_pairs: one block per pair index")
+        self._check(self._L.gb200_set_integrals_pairs(self._h, _ptr(V), _ptr(ids), len(ids), 0, None))
 
     def set_q0_correction(self, AqQ, q_abs, madelung: float):
         """The "extrapolate" q -> 0 correction (AqQ [nk, NQ] complex, q_abs [nk]); AqQ=None turns it off."""

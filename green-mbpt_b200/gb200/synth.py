@@ -147,36 +147,70 @@ def make_config(name: str, seed: int = 0, **over) -> System:
     return make_system(**kw)
 
 
+PAIR_BLOCK = 32  # stored pairs per seeded block of the device generator
+
+
+def _device_pair_block(b: int, nk: int, naux: int, nao: int, seed: int, device: int):
+    """Stored pairs [b PAIR_BLOCK, (b + 1) PAIR_BLOCK) of the device generator, each block from
+    its own seed, so a pair has the same values whichever rank or chunk generates it."""
+    import torch
+
+    p0 = b * PAIR_BLOCK
+    cnt = min(PAIR_BLOCK, pair_count(nk) - p0)
+    gen = torch.Generator(device=f"cuda:{device}")
+    gen.manual_seed(int(seed) * 1000003 + b)
+    re = torch.randn((cnt, naux, nao, nao), dtype=torch.float64, device=f"cuda:{device}", generator=gen)
+    im = torch.randn((cnt, naux, nao, nao), dtype=torch.float64, device=f"cuda:{device}", generator=gen)
+    v = torch.complex(re, im) * (1.0 / np.sqrt(2.0 * naux))
+    del re, im
+    for k in range(nk):
+        p = k * (k + 1) // 2 + k  # diagonal pairs are Hermitian per Q
+        if p0 <= p < p0 + cnt:
+            blk = v[p - p0]
+            v[p - p0] = 0.5 * (blk + blk.conj().transpose(-1, -2))
+    return v.contiguous()
+
+
 def upload_device_integrals(ctx, nk: int, naux: int, nao: int, seed: int = 0, chunk_bytes: float = 2e9,
                             device: int = 0):
     """Generate V^Q_ij(k1,k2), k1 >= k2, on the GPU chunk by chunk and hand each chunk to the context.
 
     Same distribution as make_system (complex Gaussian with E|V|^2 = 1/naux, Hermitian
-    diagonal pairs); the values come from torch's seeded CUDA generator, so they differ
-    from the host generator's.  Nothing of size nk(nk+1)/2 * naux * nao^2 is ever held
-    on the host or twice on the device.
+    diagonal pairs); the values come from torch's seeded CUDA generator (one seed per block of
+    PAIR_BLOCK stored pairs), so they differ from the host generator's.  Nothing of size
+    nk(nk+1)/2 * naux * nao^2 is ever held on the host or twice on the device.
     """
     import torch
 
     npair = pair_count(nk)
     pe = naux * nao * nao
-    per_chunk = max(1, int(chunk_bytes // (pe * 16)))
-    gen = torch.Generator(device=f"cuda:{device}")
-    gen.manual_seed(seed)
-    sd = 1.0 / np.sqrt(2.0 * naux)
-    diag = {k * (k + 1) // 2 + k for k in range(nk)}
+    per_chunk = max(1, int(chunk_bytes // (pe * 16 * PAIR_BLOCK))) * PAIR_BLOCK
     for p0 in range(0, npair, per_chunk):
         cnt = min(per_chunk, npair - p0)
-        re = torch.randn((cnt, naux, nao, nao), dtype=torch.float64, device=f"cuda:{device}", generator=gen)
-        im = torch.randn((cnt, naux, nao, nao), dtype=torch.float64, device=f"cuda:{device}", generator=gen)
-        v = torch.complex(re, im) * sd
-        del re, im
-        for p in range(p0, p0 + cnt):
-            if p in diag:
-                blk = v[p - p0]
-                v[p - p0] = 0.5 * (blk + blk.conj().transpose(-1, -2))
-        v = v.contiguous()
+        v = torch.cat([_device_pair_block(b, nk, naux, nao, seed, device)
+                       for b in range(p0 // PAIR_BLOCK, (p0 + cnt + PAIR_BLOCK - 1) // PAIR_BLOCK)])
         torch.cuda.synchronize(device)  # the context copies on its own stream
         ctx.set_integrals_device(v.data_ptr(), p0, cnt)
         torch.cuda.synchronize(device)
         del v
+
+
+def upload_device_integral_pairs(ctx, nk: int, naux: int, nao: int, pair_ids, seed: int = 0, device: int = 0):
+    """The stored pairs `pair_ids` (increasing) of upload_device_integrals' generator, and only
+    those, as the context's q-sharded integral set (gb200_set_integrals_pairs)."""
+    import torch
+
+    ids = np.asarray(pair_ids, dtype=np.int64)
+    pe = naux * nao * nao
+    out = torch.empty((len(ids), naux, nao, nao), dtype=torch.complex128, device=f"cuda:{device}")
+    blocks = ids // PAIR_BLOCK
+    for b in np.unique(blocks):
+        sel = np.nonzero(blocks == b)[0]
+        v = _device_pair_block(int(b), nk, naux, nao, seed, device)
+        out[torch.from_numpy(sel).to(out.device)] = v[torch.from_numpy(ids[sel] - b * PAIR_BLOCK).to(out.device)]
+        del v
+    torch.cuda.synchronize(device)
+    ctx.set_integrals_pairs(out.data_ptr(), ids)
+    torch.cuda.synchronize(device)
+    del out
+    return len(ids) * pe * 16

@@ -101,6 +101,22 @@ int gb200_set_integrals_device(gb200_context* ctx, int which, const double* V_de
  * (the allreduce of :53-54).  Default: all q. */
 int gb200_set_q_range(gb200_context* ctx, int q_begin, int q_end);
 
+/* q-sharded storage of the GW integrals: only the stored pairs `pair_ids` (indices
+ * k1*(k1+1)/2 + k2 with k1 >= k2, strictly increasing; `count` of them) with their blocks
+ * V_pairs [count, NQ, nao, nao] in that order, host memory (on_device = 0) or device memory
+ * (on_device = 1, `stream` as for gb200_set_integrals_device).  A rank whose q range is
+ * [q_begin, q_end) needs the pairs {k, k+q} of those q for every k: the reference's node split
+ * reads exactly the k-pairs of its q-points (gw_cpu_kernel.cpp:45-48,88-90,113-119 through
+ * df_integral_t::read_integrals, df_integral_t.h:64-84).  The context then holds 2 count - (diagonal
+ * pairs) blocks instead of nk^2.  gw_sigma and hf_fock refuse (GB200_ERR_STATE) a q range whose
+ * pairs are not all held.  With a pair subset and no separate HF integrals, hf_fock returns the
+ * partial Fock matrix of the q range (exchange over k' = k + q of those q; the direct and
+ * Madelung terms on the context whose range holds q = 0), so that the ranks' matrices add up to
+ * the full one.  gw_sigma_vjp needs the full pair set.  gb200_set_integrals or
+ * gb200_set_integrals_device (GW) go back to the full pair set. */
+int gb200_set_integrals_pairs(gb200_context* ctx, const double* V_pairs, const int64_t* pair_ids, int64_t count,
+                              int on_device, void* stream);
+
 /* The "extrapolate" q -> 0 treatment of the GW self-energy (q0_treatment, common_defs.h;
  * mbpt_q0_utils_t.cpp:11-178, call sites gw_cpu_kernel.cpp:58-64,267-270): with AqQ
  * [nk][NQ] (complex, the AqQ dataset of AqQ.h5) and q_abs [nk] (|q|), every gw_sigma call

@@ -59,6 +59,88 @@ def _rank_main(rank, ws, port, name, out_dir):
         dist.destroy_process_group()
 
 
+class _RecordingPairs:
+    """Half-stored integrals restricted to a pair subset: records every stored pair read and
+    refuses one outside the subset (the oracle's gw_solve stands in for the device here)."""
+
+    def __init__(self, V_half, held):
+        self.V_half, self.held, self.read = V_half, set(int(p) for p in held), set()
+
+    def pair(self, k1, k2):
+        import gw_oracle as O
+        p = O.pair_index(k1, k2)
+        if p not in self.held:
+            raise KeyError(f"pair ({k1}, {k2}) is not in this rank's subset")
+        self.read.add(p)
+        return O.HalfStoredIntegrals(self.V_half).pair(k1, k2)
+
+
+def _subset_rank_main(rank, ws, port, name, out_dir):
+    import torch
+    import torch.distributed as dist
+
+    import gw_oracle as O
+    from _systems import system
+    from gb200 import solvers
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=ws)
+    try:
+        s = system(name)
+        kp, _ = solvers.kq_maps(s.mesh)
+        q0, q1 = shard.q_shard(s.nk, ws, rank)
+        held = shard.pairs_for_q_range(kp, q0, q1)
+        ints = _RecordingPairs(s.V_half, held)
+        part = O.gw_solve(s.G, ints, O.NoSymBZ(s.mesh), s.grid.Tnt_b, s.grid.Ttn_b, s.ns, s.NQ, q_list=range(q0, q1))
+        # the rank's subset is exactly what its q range reads
+        assert ints.read == set(int(p) for p in held), (rank, sorted(set(held) - ints.read))
+        np.save(os.path.join(out_dir, f"pairs{rank}.npy"), held)
+        t = torch.from_numpy(part)
+        shard.reduce_partial_sigma(t, dist)
+        if rank == 0:
+            np.save(os.path.join(out_dir, "sigma.npy"), t.numpy())
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("name,ws", [("small", 2), ("odd_mesh", 2)])
+def test_rank_pair_subsets_match_reads(tmp_path, name, ws):
+    """Per-rank integral storage for the q split: each gloo rank keeps only
+    shard.pairs_for_q_range of its q range, the oracle's GW sweep over that range reads exactly
+    those pairs (no more, no fewer), the partial self-energies still sum to the full one, and
+    together the ranks hold every stored pair."""
+    import torch.multiprocessing as mp
+
+    import gw_oracle as O
+    from _systems import system
+
+    mp.start_processes(_subset_rank_main, args=(ws, _free_port(), name, str(tmp_path)), nprocs=ws, join=True,
+                       start_method="spawn")
+    s = system(name)
+    full = O.gw_solve(s.G, O.HalfStoredIntegrals(s.V_half), O.NoSymBZ(s.mesh), s.grid.Tnt_b, s.grid.Ttn_b, s.ns, s.NQ)
+    got = np.load(tmp_path / "sigma.npy")
+    assert np.abs(got - full).max() <= 1e-12 * np.abs(full).max()
+    union = set()
+    for r in range(ws):
+        union |= set(np.load(tmp_path / f"pairs{r}.npy").tolist())
+    assert union == set(range(s.nk * (s.nk + 1) // 2))
+
+
+def test_pair_subset_sizes():
+    """At nk = 125 (5x5x5) and 8 ranks each rank keeps 20-26% of the ordered blocks (the q and
+    -q of its range read the same pairs only when both are in the range)."""
+    from gb200 import solvers
+    kp, _ = solvers.kq_maps((5, 5, 5))
+    for r in range(8):
+        q0, q1 = shard.q_shard(125, 8, r)
+        ids = shard.pairs_for_q_range(kp, q0, q1)
+        assert np.all(np.diff(ids) > 0)
+        frac = shard.integral_blocks_held(ids, 125) / 125 ** 2
+        assert 0.19 < frac < 0.27, (r, frac)
+    assert shard.integral_blocks_held(shard.pairs_for_q_range(kp, 0, 125), 125) == 125 ** 2
+
+
 @pytest.mark.parametrize("name,ws", [("small", 2), ("odd_mesh", 2)])
 def test_sharded_sigma_sums_to_full(tmp_path, name, ws):
     import torch.multiprocessing as mp

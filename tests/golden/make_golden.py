@@ -88,6 +88,7 @@ def extract(ref_root: str, case: str, intdir: str = "df_hf_int") -> dict:
         trans_pairs_list=sym("pairs/trans_pairs_list"),
         kpair_irre_list=sym("pairs/kpair_irre_list"),
         Sigma1=_cplx(dat.read("result/Sigma1")),
+        k_frac=np.asarray(sym("k/mesh_scaled"), dtype=np.float64).reshape(nk, 3),
     )
     return out
 

@@ -591,10 +591,12 @@ def main_newton(args):
 def main_batch(args):
     """--batch N: N independent systems of uneven sizes (gb200.batch.uneven_systems: nk from {8, 27, 64},
     nao ~ U{8..48}, naux ~ U{4 nao..6 nao}, ntau = 80, beta = 100), integrals generated on the device,
-    one context and stream per system with memory budgets in proportion to their intermediates, the
-    self-energies issued together from a thread pool in split precision.  Prints the aggregate
-    self-energy evaluations per second (device-synchronised wall time of the whole batch) and each
-    system's max|dSigma| against its own FP64 self-energy."""
+    one context per system with memory budgets in proportion to their intermediates, tile widths from
+    the autotuner's table (gb200/tile_table.json), split precision.  The timed call is
+    gb200_gw_sigma_batch_device: the systems' q-points in step, every contraction stage one grouped
+    persistent tensor-core launch over the tiles of all systems (CUDA events).  The same batch issued
+    from a thread pool of per-system calls is timed beside it.  Prints the aggregate self-energy
+    evaluations per second and each system's max|dSigma| against its own FP64 self-energy."""
     import torch
 
     from gb200 import batch, lib, solvers, synth
@@ -613,35 +615,55 @@ def main_batch(args):
         c.set_precision(lib.PREC_SPLIT, args.slices)
         ctxs.append(c)
     b = batch.SystemBatch(ctxs)
+    widths = b.apply_tiles()
     # budgets cover the k-block intermediates; their INT8 planes take about 2S/16 of that again
     free_b, _ = torch.cuda.mem_get_info(0)
     b.share_memory(0.4 * free_b)
     G = [torch.from_numpy(s.G).cuda() for s in systems]
     Sig = [torch.empty_like(x) for x in G]
     gp, sp = [x.data_ptr() for x in G], [x.data_ptr() for x in Sig]
-    for _ in range(args.warmup):
-        b.run_gw(gp, sp)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        b.run_gw(gp, sp)
-    torch.cuda.synchronize()
-    sec = (time.perf_counter() - t0) / args.steps
+
+    def timed(run):
+        for _ in range(args.warmup):
+            run()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        t0 = time.perf_counter()
+        ev[0].record()
+        for _ in range(args.steps):
+            run()
+        ev[1].record()
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / 1e3 / args.steps, (time.perf_counter() - t0) / args.steps
+
+    grouped_s, grouped_wall = timed(lambda: b.run_gw_grouped(gp, sp))
+    grouped = [x.clone() for x in Sig]
+    _, pool_wall = timed(lambda: b.run_gw(gp, sp))
     rows = []
-    for c, s, g_, x in zip(ctxs, systems, G, Sig):
+    for c, s, g_, x, y in zip(ctxs, systems, G, grouped, Sig):
         c.set_precision(lib.PREC_FP64, args.slices)
         ref = torch.empty_like(x)
         c.gw_sigma_device(g_.data_ptr(), ref.data_ptr())
         torch.cuda.synchronize()
-        rows.append({"nk": s.nk, "nao": s.nao, "naux": s.NQ, "max_abs_dSigma": float((x - ref).abs().max()),
-                     "max_abs_Sigma": float(ref.abs().max())})
+        rows.append({"nk": s.nk, "nao": s.nao, "naux": s.NQ, "tile": c_width(widths, len(rows)),
+                     "max_abs_dSigma": float((x - ref).abs().max()), "max_abs_Sigma": float(ref.abs().max()),
+                     "grouped_equals_individual": bool(torch.equal(x, y))})
         del ref
     print(json.dumps({"workload": f"{args.batch} uneven systems (nk from {{8, 27, 64}}, nao ~ U{{8..48}}, "
                                   f"naux ~ U{{4 nao..6 nao}}, ntau = 80, beta = 100), seed {args.seed}",
-                      "precision": f"split, {args.slices} INT8 slices", "sigma_evals_per_s": args.batch / sec,
-                      "seconds_per_batch": sec, "timing": "device-synchronised wall time of the whole batch",
+                      "precision": f"split, {args.slices} INT8 slices", "sigma_evals_per_s": args.batch / grouped_s,
+                      "seconds_per_batch": grouped_s,
+                      "timing": "CUDA events around gb200_gw_sigma_batch_device (grouped launches), "
+                                f"mean of {args.steps} after {args.warmup} warm-up",
+                      "wall_seconds_per_batch": grouped_wall,
+                      "thread_pool_seconds_per_batch": pool_wall,
+                      "tile_widths": "gb200/tile_table.json (0: widest)",
                       "systems": rows}), flush=True)
     b.close()
+
+
+def c_width(widths, i):
+    return int(widths[i]) if i < len(widths) else 0
 
 
 def main_reference(args):

@@ -315,6 +315,37 @@ int gb200_gw_sigma_device(gb200_context* ctx, const double* G_dev, double* Sigma
   });
 }
 
+int gb200_gw_sigma_batch_device(gb200_context* const* ctxs, int n, const double* const* G_dev,
+                                double* const* Sigma_dev, void* stream) {
+  if (!ctxs || n <= 0 || !ctxs[0]) {
+    set_thread_error("gw_sigma_batch_device: no contexts");
+    return GB200_ERR_INVALID;
+  }
+  return guarded(ctxs[0], [&](Context& c0) {
+    require(G_dev && Sigma_dev, GB200_ERR_INVALID, "gw_sigma_batch_device: null pointer");
+    std::vector<Context*> cs;
+    std::vector<const cplx*> G;
+    std::vector<cplx*> Sg;
+    for (int i = 0; i < n; ++i) {
+      require(ctxs[i] && G_dev[i] && Sigma_dev[i], GB200_ERR_INVALID, "gw_sigma_batch_device: null pointer");
+      Context* c = reinterpret_cast<Context*>(ctxs[i]);
+      require(c->device == c0.device, GB200_ERR_INVALID, "gw_sigma_batch_device: contexts on different devices");
+      cs.push_back(c);
+      G.push_back(reinterpret_cast<const cplx*>(G_dev[i]));
+      Sg.push_back(reinterpret_cast<cplx*>(Sigma_dev[i]));
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : c0.stream;
+    gw_sigma_batch(cs, G, Sg, st);
+  });
+}
+
+int gb200_set_tile_width(gb200_context* ctx, int bn) {
+  return guarded(ctx, [&](Context& c) {
+    require(bn >= 0 && bn <= 256, GB200_ERR_INVALID, "set_tile_width: 0 (widest) or a width up to 256");
+    c.tile_bn = bn;
+  });
+}
+
 int gb200_gw_sigma_vjp(gb200_context* ctx, const double* G, const double* Sb, double* Gb, double* Vb) {
   return guarded(ctx, [&](Context& c) {
     require(G && Sb && Gb, GB200_ERR_INVALID, "gw_sigma_vjp: null pointer");

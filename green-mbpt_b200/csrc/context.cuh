@@ -88,6 +88,7 @@ struct Context {
     return std::min(cap, free_share * (double)free_b);
   }
   int split_core = 0;             // 0: tcgen05 tensor cores, 1: CUDA-core validation core
+  int tile_bn = 0;                // column tile of the split contractions (0: the widest that fits)
   SplitEngine* split = nullptr;
 
   bool have_kq = false, have_grid = false, have_V = false, have_Vhf = false, have_H = false;
@@ -152,6 +153,11 @@ void build_subset_tables(Context& c);
 // GB200_ERR_STATE unless V holds every pair the q-points [q0, q1) read: (k, k+q) and (k, k-q)
 void require_q_pairs(const Context& c, int q0, int q1);
 void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st);
+// the self-energies of several contexts together: their q-points in step (round i takes the i-th
+// q-point of every context that has one, k-blocks in step), each contraction stage of the round
+// in one grouped tensor-core launch when every context runs it in split precision
+void gw_sigma_batch(const std::vector<Context*>& cs, const std::vector<const cplx*>& G, const std::vector<cplx*>& Sigma,
+                    cudaStream_t st);
 // Gb = d/dG of Re sum conj(Sb) Sigma(G, V) (FP64; no two-component input, no q -> 0 correction);
 // with Vb non-null also d/dV on the full pair set [nk][nk][NQ][nao][nao] (zeroed here)
 void gw_sigma_vjp(Context& c, const cplx* G, const cplx* Sb, cplx* Gb, cplx* Vb, cudaStream_t st);

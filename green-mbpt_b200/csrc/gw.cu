@@ -13,6 +13,7 @@
 //    Sigma_ij = -sum V^Q_im G_mn W_QQ' conj(V^Q'_jn), in a batched order.
 #include <algorithm>
 #include <cmath>
+#include <memory>
 #include <vector>
 
 #include "context.cuh"
@@ -286,128 +287,132 @@ static void apply_q0(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
   GB_CHECK_LAUNCH();
 }
 
-void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
-  const gb200_dims& d = c.d;
-  require(d.nts % 2 == 0, GB200_ERR_WRONG_GRID, "Number of tau points should be even!!!");
-  require(c.have_kq && c.have_grid && c.have_V, GB200_ERR_STATE, "gw_sigma: k/q maps, grid and integrals must be set");
-  // two-component input: the contractions run over the 4 spin blocks of G (pseudo spins,
-  // gw_cpu_kernel.cpp:166-168,326-327) on a repacked copy, prefactor 1
-  const bool x2c = c.x2c();
-  const int nk = d.nk, ns = c.ns_eff(), nts = d.nts, nth = nts / 2, NQ = d.NQ, nw_b = d.nw_b;
-  const int64_t nao = d.nao, nao2 = nao * nao;
-  const int64_t pe = c.pair_elems();
-  const int64_t ge = nao2;                         // one G matrix
-  const int64_t g_s = (int64_t)nk * ge;            // stride of spin in G
-  const int64_t g_t = (int64_t)ns * g_s;           // stride of tau in G
-  const double pref = (d.ns == 2 || x2c) ? 1.0 : 2.0;  // gw_cpu_kernel.cpp:167
-  cplx* Sigma_out = Sigma;
-  const cplx* G_in = G;
-  const cplx* Gbar = G;  // the operand of Gbar(beta - tau, k): block (b,a) for two-component input
-  if (x2c) {
-    const int64_t n = (int64_t)nts * 4 * nk * nao2;
-    cplx* Gab = (cplx*)c.scratch.get(SL_X2C_GAB, (size_t)n * sizeof(cplx));
-    cplx* Gba = (cplx*)c.scratch.get(SL_X2C_GBA, (size_t)n * sizeof(cplx));
-    x2c_pack_g_kernel<<<grid_for(n, 256), 256, 0, st>>>(G, Gab, Gba, nts, nk, (int)nao);
-    GB_CHECK_LAUNCH();
-    G = Gab;
-    Gbar = Gba;
-    Sigma = (cplx*)c.scratch.get(SL_X2C_SIG, (size_t)n * sizeof(cplx));
-  }
-  const bool split = c.prec_mode == GB200_PREC_SPLIT;
+namespace {
 
-  for (int i = 0; i < 5; ++i)
-    if (!c.ev[i]) GB_CUDA(cudaEventCreate(&c.ev[i]));
-  GB_CUDA(cudaEventRecord(c.ev[0], st));
+// One GW self-energy evaluation of a context, in the steps that the single-system loop and the
+// batched loop both drive: per q-point the P0 contractions of each k-block, the aux-basis solve,
+// and the Sigma contractions of each k-block (gw_cpu_kernel.cpp:31-72,74-134).
+struct GwRun {
+  Context& c;
+  cudaStream_t st;
+  const gb200_dims& d;
+  bool x2c;
+  int nk, ns, nts, nth, NQ, nw_b;
+  int64_t nao, nao2, pe, ge, g_s, g_t;
+  double pref;
+  cplx* Sigma_out;
+  const cplx* G_in;
+  const cplx* G;
+  const cplx* Gbar;  // the operand of Gbar(beta - tau, k): block (b,a) for two-component input
+  cplx* Sigma;
+  int kb = 1;
+  int64_t per_k_sigma = 0;
+  cplx *P0 = nullptr, *Pw = nullptr, *Pinv = nullptr, *aug = nullptr, *X1 = nullptr, *X2 = nullptr;
+  int q0 = 0, q1 = 0;
 
-  GB_CUDA(cudaMemsetAsync(Sigma, 0, (size_t)nts * ns * nk * nao2 * sizeof(cplx), st));
-  const int64_t per_k_sigma = (int64_t)nts * ns * pe;
-  const int kb = choose_kblock(c, per_k_sigma);
-  cplx* P0 = (cplx*)c.scratch.get(SL_P0, (size_t)nts * NQ * NQ * sizeof(cplx));
-  cplx* Pw = (cplx*)c.scratch.get(SL_PW, (size_t)nw_b * NQ * NQ * sizeof(cplx));
-  cplx* Pinv = (cplx*)c.scratch.get(SL_PINV, (size_t)nw_b * NQ * NQ * sizeof(cplx));
-  cplx* aug = (cplx*)c.scratch.get(SL_AUG, (size_t)nw_b * NQ * 2 * NQ * sizeof(cplx));
-  cplx* X1 = (cplx*)c.scratch.get(SL_Y1, (size_t)kb * per_k_sigma * sizeof(cplx));
-  cplx* X2 = (cplx*)c.scratch.get(SL_Y2, (size_t)kb * per_k_sigma * sizeof(cplx));
-  SplitEngine* se = split ? split_engine(c) : nullptr;
-  // the P0 and Sigma contractions run in the selected precision; the
-  // transforms and the aux-basis solve always run in FP64
-  auto contract = [&](const ZGemm& g, int stage) {
-    if (se) split_gemm(c, *se, g, st, c.contraction_slices[stage]);
-    else zgemm_fp64(g, st);
-  };
-
-  float t_p0 = 0, t_w = 0, t_sig = 0;
-  if (c.q0_on) {
-    require(c.q_begin <= 0 && (c.q_end < 0 || c.q_end >= nk), GB200_ERR_INVALID,
-            "q0 correction: needs all q-points in one context (it extrapolates over q)");
-    c.eps_inv.alloc((size_t)nw_b * nk);
-  }
-  // this context's share of the q loop (gw_cpu_kernel.cpp:45 distributes q over nodes the same way);
-  // the partial Sigma is already divided by nk, so shards sum to the full self-energy
-  const int q0 = std::max(0, c.q_begin);
-  const int q1 = c.q_end < 0 ? nk : std::min(nk, c.q_end);
-  require_q_pairs(c, q0, q1);
-  // stage timings: events recorded on the stream and read after the loop, so the host never
-  // waits inside it
-  const size_t nev = (size_t)std::max(0, q1 - q0) * 4;
-  while (c.qev.size() < nev) {
-    cudaEvent_t e;
-    GB_CUDA(cudaEventCreate(&e));
-    c.qev.push_back(e);
-  }
-  for (int q = q0; q < q1; ++q) {
-    cudaEvent_t* qe = c.qev.data() + (size_t)(q - q0) * 4;
-    // ---------------- polarization P0(tau, q), tau in the first half ---------
-    GB_CUDA(cudaEventRecord(qe[0], st));
-    GB_CUDA(cudaMemsetAsync(P0, 0, (size_t)nts * NQ * NQ * sizeof(cplx), st));
-    for (int k0 = 0; k0 < nk; k0 += kb) {
-      const int kbk = std::min(kb, nk - k0);
-      const int64_t* tVp = c.tab_pair_plus.get() + (int64_t)q * nk + k0;
-      const int64_t* tGp = c.tab_g_plus.get() + (int64_t)q * nk + k0;
-      const int64_t blkT1 = (int64_t)nth * ns * pe;  // per kk in T1
-      // (a) T1[kk][t][s][(Q,p)][n] = sum_m V(k,k+q)[(Q,p)][m] G(t,s,k+q)[m][n], computed as its
-      //     transpose T1^T = G^T V^T so that the large operand V is the right (column) operand:
-      //     rows ((t,s),n) (M = nth*ns*nao), columns (Q,p) (N = NQ*nao), K = m
-      ZGemm a;
-      a.M = (int64_t)nth * ns * nao; a.N = (int64_t)NQ * nao; a.K = nao;
-      a.nb0 = kbk;
-      a.A.ptr = G; a.A.row = two(nao, 1, g_s); a.A.col = lin(nao); a.A.bat.tab0 = tGp;
-      a.B.ptr = c.V.get(); a.B.row = lin(1); a.B.col = lin(nao); a.B.bat.tab0 = tVp;
-      a.C.ptr = X1; a.C.row = two(nao, 1, pe); a.C.col = lin(nao);
-      a.C.bat.s0 = blkT1;
-      // (b) Bt[t][kk][s][Q][r][n] = sum_p Gbar(nts-1-t, s, k)[r][p] T1[kk][t][s][Q][p][n]
-      ZGemm b;
-      b.M = nao; b.N = (int64_t)NQ * nao; b.K = nao;
-      b.nb0 = kbk; b.nb1 = nth; b.nb2 = ns;
-      b.A = dense(Gbar + (int64_t)(nts - 1) * g_t + (int64_t)k0 * ge, nao);
-      b.A.bat.s0 = ge; b.A.bat.s1 = -g_t; b.A.bat.s2 = g_s;
-      b.B.ptr = X1; b.B.row = lin(nao); b.B.col = two(nao, 1, nao2);
-      b.B.bat.s0 = blkT1; b.B.bat.s1 = (int64_t)ns * pe; b.B.bat.s2 = pe;
-      b.C.ptr = X2; b.C.row = lin(nao); b.C.col = two(nao, 1, nao2);
-      b.C.bat.s0 = (int64_t)ns * pe; b.C.bat.s1 = (int64_t)kbk * ns * pe; b.C.bat.s2 = pe;
-      // (c) P0[t][Q][Q'] -= pref sum_{(kk,s),(r,n)} Bt[t][(kk,s)][Q][(r,n)] conj(V(k,k+q)[Q'][(r,n)]),
-      //     computed as P0^T = conj(V) Bt^T: the tau-independent V is the left operand (sliced
-      //     once per call), Bt the right one; rows Q', columns Q, K = ((kk,s),(r,n))
-      ZGemm cc;
-      cc.M = NQ; cc.N = NQ; cc.K = (int64_t)kbk * ns * nao2;
-      cc.nb0 = 1; cc.nb1 = 1; cc.nb2 = nth;
-      cc.A.ptr = c.V.get(); cc.A.row = lin(nao2); cc.A.conj = true;
-      cc.A.col = twotab(nao2, 1, c.tab_pair_plus_ns.get() + ((int64_t)q * nk + k0) * ns);
-      cc.B.ptr = X2; cc.B.col = lin(nao2); cc.B.row = two(nao2, 1, (int64_t)NQ * nao2);
-      cc.B.bat.s2 = (int64_t)kbk * ns * pe;
-      cc.C.ptr = P0; cc.C.row = lin(1); cc.C.col = lin(NQ); cc.C.bat.s2 = (int64_t)NQ * NQ;
-      cc.alpha = cmk(-pref, 0.0); cc.beta = cmk(1.0, 0.0);
-      contract(a, 0);
-      contract(b, 1);
-      contract(cc, 2);
+  GwRun(Context& c_, const cplx* G_, cplx* Sigma_, cudaStream_t st_) : c(c_), st(st_), d(c_.d) {
+    require(d.nts % 2 == 0, GB200_ERR_WRONG_GRID, "Number of tau points should be even!!!");
+    require(c.have_kq && c.have_grid && c.have_V, GB200_ERR_STATE, "gw_sigma: k/q maps, grid and integrals must be set");
+    // two-component input: the contractions run over the 4 spin blocks of G (pseudo spins,
+    // gw_cpu_kernel.cpp:166-168,326-327) on a repacked copy, prefactor 1
+    x2c = c.x2c();
+    nk = d.nk; ns = c.ns_eff(); nts = d.nts; nth = nts / 2; NQ = d.NQ; nw_b = d.nw_b;
+    nao = d.nao; nao2 = nao * nao;
+    pe = c.pair_elems();
+    ge = nao2;                      // one G matrix
+    g_s = (int64_t)nk * ge;         // stride of spin in G
+    g_t = (int64_t)ns * g_s;        // stride of tau in G
+    pref = (d.ns == 2 || x2c) ? 1.0 : 2.0;  // gw_cpu_kernel.cpp:167
+    Sigma_out = Sigma_;
+    G_in = G_;
+    G = G_;
+    Gbar = G_;
+    Sigma = Sigma_;
+    if (x2c) {
+      const int64_t n = (int64_t)nts * 4 * nk * nao2;
+      cplx* Gab = (cplx*)c.scratch.get(SL_X2C_GAB, (size_t)n * sizeof(cplx));
+      cplx* Gba = (cplx*)c.scratch.get(SL_X2C_GBA, (size_t)n * sizeof(cplx));
+      x2c_pack_g_kernel<<<grid_for(n, 256), 256, 0, st>>>(G_, Gab, Gba, nts, nk, (int)nao);
+      GB_CHECK_LAUNCH();
+      G = Gab;
+      Gbar = Gba;
+      Sigma = (cplx*)c.scratch.get(SL_X2C_SIG, (size_t)n * sizeof(cplx));
     }
-    {
+    GB_CUDA(cudaMemsetAsync(Sigma, 0, (size_t)nts * ns * nk * nao2 * sizeof(cplx), st));
+    per_k_sigma = (int64_t)nts * ns * pe;
+    kb = choose_kblock(c, per_k_sigma);
+    P0 = (cplx*)c.scratch.get(SL_P0, (size_t)nts * NQ * NQ * sizeof(cplx));
+    Pw = (cplx*)c.scratch.get(SL_PW, (size_t)nw_b * NQ * NQ * sizeof(cplx));
+    Pinv = (cplx*)c.scratch.get(SL_PINV, (size_t)nw_b * NQ * NQ * sizeof(cplx));
+    aug = (cplx*)c.scratch.get(SL_AUG, (size_t)nw_b * NQ * 2 * NQ * sizeof(cplx));
+    X1 = (cplx*)c.scratch.get(SL_Y1, (size_t)kb * per_k_sigma * sizeof(cplx));
+    X2 = (cplx*)c.scratch.get(SL_Y2, (size_t)kb * per_k_sigma * sizeof(cplx));
+    if (c.q0_on) {
+      require(c.q_begin <= 0 && (c.q_end < 0 || c.q_end >= nk), GB200_ERR_INVALID,
+              "q0 correction: needs all q-points in one context (it extrapolates over q)");
+      c.eps_inv.alloc((size_t)nw_b * nk);
+    }
+    // this context's share of the q loop (gw_cpu_kernel.cpp:45 distributes q over nodes the same
+    // way); the partial Sigma is already divided by nk, so shards sum to the full self-energy
+    q0 = std::max(0, c.q_begin);
+    q1 = c.q_end < 0 ? nk : std::min(nk, c.q_end);
+    require_q_pairs(c, q0, q1);
+  }
+
+  int nkblocks() const { return (nk + kb - 1) / kb; }
+
+  // ---------------- polarization P0(tau, q), tau in the first half ---------
+  void p0_begin(int) { GB_CUDA(cudaMemsetAsync(P0, 0, (size_t)nts * NQ * NQ * sizeof(cplx), st)); }
+
+  void p0_gemms(int q, int k0, ZGemm (&out)[3]) {
+    const int kbk = std::min(kb, nk - k0);
+    const int64_t* tVp = c.tab_pair_plus.get() + (int64_t)q * nk + k0;
+    const int64_t* tGp = c.tab_g_plus.get() + (int64_t)q * nk + k0;
+    const int64_t blkT1 = (int64_t)nth * ns * pe;  // per kk in T1
+      // (a) T1[kk][t][s][(Q,p)][n] = sum_m V(k,k+q)[(Q,p)][m] G(t,s,k+q)[m][n], computed as its
+    //     transpose T1^T = G^T V^T so that the large operand V is the right (column) operand:
+    //     rows ((t,s),n) (M = nth*ns*nao), columns (Q,p) (N = NQ*nao), K = m
+    ZGemm a;
+    a.M = (int64_t)nth * ns * nao; a.N = (int64_t)NQ * nao; a.K = nao;
+    a.nb0 = kbk;
+    a.A.ptr = G; a.A.row = two(nao, 1, g_s); a.A.col = lin(nao); a.A.bat.tab0 = tGp;
+    a.B.ptr = c.V.get(); a.B.row = lin(1); a.B.col = lin(nao); a.B.bat.tab0 = tVp;
+    a.C.ptr = X1; a.C.row = two(nao, 1, pe); a.C.col = lin(nao);
+    a.C.bat.s0 = blkT1;
+    // (b) Bt[t][kk][s][Q][r][n] = sum_p Gbar(nts-1-t, s, k)[r][p] T1[kk][t][s][Q][p][n]
+    ZGemm b;
+    b.M = nao; b.N = (int64_t)NQ * nao; b.K = nao;
+    b.nb0 = kbk; b.nb1 = nth; b.nb2 = ns;
+    b.A = dense(Gbar + (int64_t)(nts - 1) * g_t + (int64_t)k0 * ge, nao);
+    b.A.bat.s0 = ge; b.A.bat.s1 = -g_t; b.A.bat.s2 = g_s;
+    b.B.ptr = X1; b.B.row = lin(nao); b.B.col = two(nao, 1, nao2);
+    b.B.bat.s0 = blkT1; b.B.bat.s1 = (int64_t)ns * pe; b.B.bat.s2 = pe;
+    b.C.ptr = X2; b.C.row = lin(nao); b.C.col = two(nao, 1, nao2);
+    b.C.bat.s0 = (int64_t)ns * pe; b.C.bat.s1 = (int64_t)kbk * ns * pe; b.C.bat.s2 = pe;
+    // (c) P0[t][Q][Q'] -= pref sum_{(kk,s),(r,n)} Bt[t][(kk,s)][Q][(r,n)] conj(V(k,k+q)[Q'][(r,n)]),
+    //     computed as P0^T = conj(V) Bt^T: the tau-independent V is the left operand (sliced
+    //     once per call), Bt the right one; rows Q', columns Q, K = ((kk,s),(r,n))
+    ZGemm cc;
+    cc.M = NQ; cc.N = NQ; cc.K = (int64_t)kbk * ns * nao2;
+    cc.nb0 = 1; cc.nb1 = 1; cc.nb2 = nth;
+    cc.A.ptr = c.V.get(); cc.A.row = lin(nao2); cc.A.conj = true;
+    cc.A.col = twotab(nao2, 1, c.tab_pair_plus_ns.get() + ((int64_t)q * nk + k0) * ns);
+    cc.B.ptr = X2; cc.B.col = lin(nao2); cc.B.row = two(nao2, 1, (int64_t)NQ * nao2);
+    cc.B.bat.s2 = (int64_t)kbk * ns * pe;
+    cc.C.ptr = P0; cc.C.row = lin(1); cc.C.col = lin(NQ); cc.C.bat.s2 = (int64_t)NQ * NQ;
+    cc.alpha = cmk(-pref, 0.0); cc.beta = cmk(1.0, 0.0);
+    out[0] = a;
+    out[1] = b;
+    out[2] = cc;
+  }
+
+  // ---------------- screened interaction (gw_cpu_kernel.cpp:227-279) -------
+  void w_solve(int q) {
+    {  // P0 = herm(P0 / nk), P0(beta - tau) = P0(tau) (gw_cpu_kernel.cpp:217-225)
       int64_t total = (int64_t)nth * NQ * (NQ + 1) / 2;
       symmetrize_p0_kernel<<<grid_for(total, 256), 256, 0, st>>>(P0, nts, NQ, 1.0 / nk);
       GB_CHECK_LAUNCH();
     }
-    GB_CUDA(cudaEventRecord(qe[1], st));
-    // ---------------- screened interaction (gw_cpu_kernel.cpp:227-279) -------
     {
       ZGemm f;  // Pw[n] = sum_t Tnt_b[n][t] P0[t]
       f.M = nw_b; f.N = (int64_t)NQ * NQ; f.K = nts;
@@ -449,68 +454,122 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
       bt.C.ptr = P0; bt.C.row = lin((int64_t)NQ * NQ); bt.C.col = lin(1);
       zgemm_fp64(bt, st);
     }
-    GB_CUDA(cudaEventRecord(qe[2], st));
-    // ---------------- self-energy contribution of this q ---------------------
-    for (int k0 = 0; k0 < nk; k0 += kb) {
-      const int kbk = std::min(kb, nk - k0);
-      const int64_t* tVm = c.tab_pair_minus.get() + (int64_t)q * nk + k0;
-      const int64_t* tGm = c.tab_g_minus.get() + (int64_t)q * nk + k0;
-      const int64_t blk = (int64_t)nts * ns * pe;  // per kk in Y1 / Y2
+  }
+
+  // ---------------- self-energy contribution of this q ---------------------
+  void sigma_gemms(int q, int k0, ZGemm (&out)[3]) {
+    const int kbk = std::min(kb, nk - k0);
+    const int64_t* tVm = c.tab_pair_minus.get() + (int64_t)q * nk + k0;
+    const int64_t* tGm = c.tab_g_minus.get() + (int64_t)q * nk + k0;
+    const int64_t blk = (int64_t)nts * ns * pe;  // per kk in Y1 / Y2
       // (d) Y1[kk][t][s][(Q,i)][n] = sum_m V(k,k-q)[(Q,i)][m] G(t,s,k-q)[m][n], as its transpose
-      //     (V the right operand): rows ((t,s),n), columns (Q,i), K = m
-      ZGemm dd;
-      dd.M = (int64_t)nts * ns * nao; dd.N = (int64_t)NQ * nao; dd.K = nao;
-      dd.nb0 = kbk;
-      dd.A.ptr = G; dd.A.row = two(nao, 1, g_s); dd.A.col = lin(nao); dd.A.bat.tab0 = tGm;
-      dd.B.ptr = c.V.get(); dd.B.row = lin(1); dd.B.col = lin(nao); dd.B.bat.tab0 = tVm;
-      dd.C.ptr = X1; dd.C.row = two(nao, 1, pe); dd.C.col = lin(nao);
-      dd.C.bat.s0 = blk;
-      // (e) Y2[kk][t][s][(i,n)][Q'] = sum_Q Y1[kk][t][s][Q][(i,n)] W(t)[Q][Q'], as Y2^T = W^T Y1:
-      //     the small W(t) is the left operand, Y1 the right one; rows Q', columns (kk,(i,n)), K = Q
-      ZGemm e;
-      e.M = NQ; e.N = (int64_t)kbk * nao2; e.K = NQ;
-      e.nb0 = 1; e.nb1 = nts; e.nb2 = ns;
-      e.A.ptr = P0; e.A.row = lin(1); e.A.col = lin(NQ); e.A.bat.s1 = (int64_t)NQ * NQ;
-      e.B.ptr = X1; e.B.row = lin(nao2); e.B.col = two(nao2, 1, blk);
-      e.B.bat.s1 = (int64_t)ns * pe; e.B.bat.s2 = pe;
-      e.C.ptr = X2; e.C.row = lin(1); e.C.col = two(nao2, NQ, blk);
-      e.C.bat.s1 = (int64_t)ns * pe; e.C.bat.s2 = pe;
-      // (f) Sigma[t][s][k][i][j] -= sum_{(n,Q')} Y2[kk][t][s][i][(n,Q')] conj(V(k,k-q)[Q'][j][n]), as
-      //     Sigma^T = conj(V) Y2^T: rows j (M = nao), columns ((t,s),i) (N = nts*ns*nao),
-      //     K = (n,Q'); the large Y2 is the right operand
-      ZGemm f;
-      f.M = nao; f.N = (int64_t)nts * ns * nao; f.K = nao * NQ;
-      f.nb0 = kbk;
-      f.A.ptr = c.V.get(); f.A.row = lin(nao); f.A.col = two(NQ, nao2, 1); f.A.conj = true;
-      f.A.bat.tab0 = tVm;
-      f.B.ptr = X2; f.B.row = lin(1); f.B.col = two(nao, nao * NQ, pe);
-      f.B.bat.s0 = blk;
-      f.C.ptr = Sigma + (int64_t)k0 * ge; f.C.row = lin(1); f.C.col = two(nao, nao, g_s);
-      f.C.bat.s0 = ge;
-      f.alpha = cmk(-1.0, 0.0); f.beta = cmk(1.0, 0.0);
-      contract(dd, 3);
-      contract(e, 4);
-      contract(f, 5);
+    //     (V the right operand): rows ((t,s),n), columns (Q,i), K = m
+    ZGemm dd;
+    dd.M = (int64_t)nts * ns * nao; dd.N = (int64_t)NQ * nao; dd.K = nao;
+    dd.nb0 = kbk;
+    dd.A.ptr = G; dd.A.row = two(nao, 1, g_s); dd.A.col = lin(nao); dd.A.bat.tab0 = tGm;
+    dd.B.ptr = c.V.get(); dd.B.row = lin(1); dd.B.col = lin(nao); dd.B.bat.tab0 = tVm;
+    dd.C.ptr = X1; dd.C.row = two(nao, 1, pe); dd.C.col = lin(nao);
+    dd.C.bat.s0 = blk;
+    // (e) Y2[kk][t][s][(i,n)][Q'] = sum_Q Y1[kk][t][s][Q][(i,n)] W(t)[Q][Q'], as Y2^T = W^T Y1:
+    //     the small W(t) is the left operand, Y1 the right one; rows Q', columns (kk,(i,n)), K = Q
+    ZGemm e;
+    e.M = NQ; e.N = (int64_t)kbk * nao2; e.K = NQ;
+    e.nb0 = 1; e.nb1 = nts; e.nb2 = ns;
+    e.A.ptr = P0; e.A.row = lin(1); e.A.col = lin(NQ); e.A.bat.s1 = (int64_t)NQ * NQ;
+    e.B.ptr = X1; e.B.row = lin(nao2); e.B.col = two(nao2, 1, blk);
+    e.B.bat.s1 = (int64_t)ns * pe; e.B.bat.s2 = pe;
+    e.C.ptr = X2; e.C.row = lin(1); e.C.col = two(nao2, NQ, blk);
+    e.C.bat.s1 = (int64_t)ns * pe; e.C.bat.s2 = pe;
+    // (f) Sigma[t][s][k][i][j] -= sum_{(n,Q')} Y2[kk][t][s][i][(n,Q')] conj(V(k,k-q)[Q'][j][n]), as
+    //     Sigma^T = conj(V) Y2^T: rows j (M = nao), columns ((t,s),i) (N = nts*ns*nao),
+    //     K = (n,Q'); the large Y2 is the right operand
+    ZGemm f;
+    f.M = nao; f.N = (int64_t)nts * ns * nao; f.K = nao * NQ;
+    f.nb0 = kbk;
+    f.A.ptr = c.V.get(); f.A.row = lin(nao); f.A.col = two(NQ, nao2, 1); f.A.conj = true;
+    f.A.bat.tab0 = tVm;
+    f.B.ptr = X2; f.B.row = lin(1); f.B.col = two(nao, nao * NQ, pe);
+    f.B.bat.s0 = blk;
+    f.C.ptr = Sigma + (int64_t)k0 * ge; f.C.row = lin(1); f.C.col = two(nao, nao, g_s);
+    f.C.bat.s0 = ge;
+    f.alpha = cmk(-1.0, 0.0); f.beta = cmk(1.0, 0.0);
+    out[0] = dd;
+    out[1] = e;
+    out[2] = f;
+  }
+
+  void finish() {
+    scale_inplace(Sigma, (int64_t)nts * ns * nk * nao2, 1.0 / nk, st);  // gw_cpu_kernel.cpp:55
+    if (x2c) {
+      const int64_t n = (int64_t)nts * 4 * nk * nao2;
+      x2c_unpack_sigma_kernel<<<grid_for(n, 256), 256, 0, st>>>(Sigma, Sigma_out, nts, nk, (int)nao);
+      GB_CHECK_LAUNCH();
+    }
+    if (c.q0_on) apply_q0(c, G_in, Sigma_out, st);
+  }
+};
+
+// slices of contraction `stage` of a context in split precision (0: FP64)
+int stage_slices(const Context& c, int stage) {
+  if (c.prec_mode != GB200_PREC_SPLIT) return 0;
+  return c.contraction_slices[stage] > 0 ? c.contraction_slices[stage] : c.slices;
+}
+
+void check_split_error(Context& c, cudaStream_t st) {
+  if (c.prec_mode != GB200_PREC_SPLIT) return;
+  int e = split_check_error(c, st);
+  require(e == 0, GB200_ERR_CUDA, "split contraction: tensor-core pipeline wait timed out (code " + std::to_string(e) + ")");
+}
+
+}  // namespace
+
+void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
+  for (int i = 0; i < 5; ++i)
+    if (!c.ev[i]) GB_CUDA(cudaEventCreate(&c.ev[i]));
+  GB_CUDA(cudaEventRecord(c.ev[0], st));
+  GwRun r(c, G, Sigma, st);
+  // the P0 and Sigma contractions run in the selected precision; the
+  // transforms and the aux-basis solve always run in FP64
+  SplitEngine* se = c.prec_mode == GB200_PREC_SPLIT ? split_engine(c) : nullptr;
+  auto contract = [&](const ZGemm& g, int stage) {
+    if (se) split_gemm(c, *se, g, st, c.contraction_slices[stage]);
+    else zgemm_fp64(g, st);
+  };
+  // stage timings: events recorded on the stream and read after the loop, so the host never
+  // waits inside it
+  const size_t nev = (size_t)std::max(0, r.q1 - r.q0) * 4;
+  while (c.qev.size() < nev) {
+    cudaEvent_t e;
+    GB_CUDA(cudaEventCreate(&e));
+    c.qev.push_back(e);
+  }
+  ZGemm g3[3];
+  for (int q = r.q0; q < r.q1; ++q) {
+    cudaEvent_t* qe = c.qev.data() + (size_t)(q - r.q0) * 4;
+    GB_CUDA(cudaEventRecord(qe[0], st));
+    r.p0_begin(q);
+    for (int k0 = 0; k0 < r.nk; k0 += r.kb) {
+      r.p0_gemms(q, k0, g3);
+      for (int i = 0; i < 3; ++i) contract(g3[i], i);
+    }
+    GB_CUDA(cudaEventRecord(qe[1], st));
+    r.w_solve(q);
+    GB_CUDA(cudaEventRecord(qe[2], st));
+    for (int k0 = 0; k0 < r.nk; k0 += r.kb) {
+      r.sigma_gemms(q, k0, g3);
+      for (int i = 0; i < 3; ++i) contract(g3[i], 3 + i);
     }
     GB_CUDA(cudaEventRecord(qe[3], st));
   }
-  scale_inplace(Sigma, (int64_t)nts * ns * nk * nao2, 1.0 / nk, st);  // gw_cpu_kernel.cpp:55
-  if (x2c) {
-    const int64_t n = (int64_t)nts * 4 * nk * nao2;
-    x2c_unpack_sigma_kernel<<<grid_for(n, 256), 256, 0, st>>>(Sigma, Sigma_out, nts, nk, (int)nao);
-    GB_CHECK_LAUNCH();
-  }
-  if (c.q0_on) apply_q0(c, G_in, Sigma_out, st);
-  if (se) {
-    int e = split_check_error(c, st);
-    require(e == 0, GB200_ERR_CUDA, "split contraction: tensor-core pipeline wait timed out (code " + std::to_string(e) + ")");
-  }
+  r.finish();
+  check_split_error(c, st);
   GB_CUDA(cudaEventRecord(c.ev[4], st));
   GB_CUDA(cudaEventSynchronize(c.ev[4]));
-  float tot = 0;
+  float tot = 0, t_p0 = 0, t_w = 0, t_sig = 0;
   GB_CUDA(cudaEventElapsedTime(&tot, c.ev[0], c.ev[4]));
-  for (int q = q0; q < q1; ++q) {
-    const cudaEvent_t* qe = c.qev.data() + (size_t)(q - q0) * 4;
+  for (int q = r.q0; q < r.q1; ++q) {
+    const cudaEvent_t* qe = c.qev.data() + (size_t)(q - r.q0) * 4;
     float a_ms = 0, b_ms = 0, c_ms = 0;
     GB_CUDA(cudaEventElapsedTime(&a_ms, qe[0], qe[1]));
     GB_CUDA(cudaEventElapsedTime(&b_ms, qe[1], qe[2]));
@@ -518,6 +577,64 @@ void gw_sigma(Context& c, const cplx* G, cplx* Sigma, cudaStream_t st) {
     t_p0 += a_ms; t_w += b_ms; t_sig += c_ms;
   }
   c.timings[0] = t_p0; c.timings[1] = t_w; c.timings[2] = t_sig; c.timings[3] = tot;
+}
+
+void gw_sigma_batch(const std::vector<Context*>& cs, const std::vector<const cplx*>& G, const std::vector<cplx*>& Sigma,
+                    cudaStream_t st) {
+  require(!cs.empty() && cs.size() == G.size() && cs.size() == Sigma.size(), GB200_ERR_INVALID,
+          "gw_sigma_batch: one G and one Sigma per context");
+  for (size_t i = 0; i < cs.size(); ++i)
+    for (size_t j = 0; j < i; ++j) require(cs[i] != cs[j], GB200_ERR_INVALID, "gw_sigma_batch: a context appears twice");
+  std::vector<std::unique_ptr<GwRun>> runs;
+  for (size_t i = 0; i < cs.size(); ++i) runs.emplace_back(new GwRun(*cs[i], G[i], Sigma[i], st));
+  // one stage of every system that takes part: a grouped tensor-core launch when all of them run
+  // that stage in split precision with the same slice count, else one contraction each
+  auto contract_all = [&](std::vector<Context*>& ctx, std::vector<ZGemm>& gs, int stage) {
+    if (gs.empty()) return;
+    const int S = stage_slices(*ctx[0], stage);
+    bool grouped = S > 0;
+    for (Context* x : ctx) grouped = grouped && stage_slices(*x, stage) == S;
+    if (grouped) {
+      split_gemm_group(ctx, gs, st, S);
+      return;
+    }
+    for (size_t i = 0; i < ctx.size(); ++i) {
+      if (stage_slices(*ctx[i], stage) > 0) split_gemm(*ctx[i], *split_engine(*ctx[i]), gs[i], st, stage_slices(*ctx[i], stage));
+      else zgemm_fp64(gs[i], st);
+    }
+  };
+  int rounds = 0;
+  for (auto& r : runs) rounds = std::max(rounds, r->q1 - r->q0);
+  // round i: the i-th q-point of every system that has one, its k-blocks in step
+  for (int i = 0; i < rounds; ++i) {
+    std::vector<GwRun*> act;
+    for (auto& r : runs)
+      if (r->q0 + i < r->q1) act.push_back(r.get());
+    int nblk = 0;
+    for (GwRun* r : act) {
+      r->p0_begin(r->q0 + i);
+      nblk = std::max(nblk, r->nkblocks());
+    }
+    for (int half = 0; half < 2; ++half) {
+      if (half == 1)
+        for (GwRun* r : act) r->w_solve(r->q0 + i);
+      for (int j = 0; j < nblk; ++j) {
+        std::vector<Context*> ctx;
+        std::vector<ZGemm> gs[3];
+        for (GwRun* r : act) {
+          if (j >= r->nkblocks()) continue;
+          ZGemm g3[3];
+          if (half == 0) r->p0_gemms(r->q0 + i, j * r->kb, g3);
+          else r->sigma_gemms(r->q0 + i, j * r->kb, g3);
+          ctx.push_back(&r->c);
+          for (int m = 0; m < 3; ++m) gs[m].push_back(g3[m]);
+        }
+        for (int m = 0; m < 3; ++m) contract_all(ctx, gs[m], 3 * half + m);
+      }
+    }
+  }
+  for (auto& r : runs) r->finish();
+  for (Context* x : cs) check_split_error(*x, st);
 }
 
 }  // namespace gb200

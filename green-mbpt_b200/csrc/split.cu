@@ -191,7 +191,43 @@ struct GemmParams {
   int alpha_pow2;  // alpha is real and a power of two (possibly negative)
   int pair;        // the chunk is short enough that diagonal pairs (0,1), (2,3) fit int32 exactly
   int* err;
+  // grouped launch: the problems' entries (tile ranges in order) and the total tile count; the
+  // launch-wide fields above (S, BN = the widest tile, stages, nbuf, err) size the shared ring
+  const struct GroupEntry* group;
+  int ngroup;
+  int64_t ntiles;
 };
+
+// one problem of a grouped launch: its tensor maps, parameters and first global tile
+struct alignas(64) GroupEntry {
+  CUtensorMap mA, mB;
+  GemmParams p;
+  int64_t tile_begin;
+};
+
+// a tile of the launch: its problem's parameters and maps, and its index within the problem
+struct TileRef {
+  const GemmParams* p;
+  const CUtensorMap* mA;
+  const CUtensorMap* mB;
+  int64_t t;
+};
+
+template <bool GROUPED>
+__device__ __forceinline__ TileRef tile_ref(const GemmParams& p, const CUtensorMap* mA, const CUtensorMap* mB, int64_t t) {
+  if constexpr (!GROUPED) {
+    return TileRef{&p, mA, mB, t};
+  } else {
+    int lo = 0, hi = p.ngroup - 1;  // last entry with tile_begin <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if (p.group[mid].tile_begin <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const GroupEntry& e = p.group[lo];
+    return TileRef{&e.p, &e.mA, &e.mB, t - e.tile_begin};
+  }
+}
 
 __device__ __forceinline__ int64_t reduced_batch(const int dep[3], int64_t b0, int64_t b1, int64_t b2, int64_t n1,
                                                  int64_t n2) {
@@ -576,7 +612,7 @@ __device__ __forceinline__ TileCoord tile_coord(const GemmParams& p, int64_t t) 
 //  warp 1       MMA issuer (one thread), `nbuf` TMEM accumulator sets of S * BN columns
 //  warps 2..    epilogue (EPI_WARPS): TMEM -> registers -> FP64 recombination -> stores to C
 // With nbuf = 2 the epilogue of one tile overlaps the MMAs of the next.
-template <int SS>
+template <int SS, bool GROUPED>
 __global__ void __launch_bounds__(NWARPS * 32, 1)
     split_gemm_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, GemmParams p) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -600,7 +636,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
   const uint32_t acc_cols = (uint32_t)(S * p.BN);
   const uint32_t need = acc_cols * (uint32_t)nbuf;
   const uint32_t ncols_alloc = need <= 32 ? 32 : need <= 64 ? 64 : need <= 128 ? 128 : need <= 256 ? 256 : 512;
-  const int64_t ntiles = (int64_t)p.tiles_m * p.tiles_n * p.nb0 * p.nb1 * p.nb2;
+  const int64_t ntiles = GROUPED ? p.ntiles : (int64_t)p.tiles_m * p.tiles_n * p.nb0 * p.nb1 * p.nb2;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < L.stages; ++s) {
@@ -626,9 +662,25 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
   if (warp == 0) {
     if (lane == 0) {
       int64_t it = 0;
+      const GemmParams* last_q = nullptr;
       for (int64_t t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x) {
-        const TileCoord tc = tile_coord(p, t);
-        for (int kb = 0; kb < p.nkb; ++kb, ++it) {
+        const TileRef tr = tile_ref<GROUPED>(p, &mapA, &mapB, t);
+        const GemmParams& q = *tr.p;
+        if constexpr (GROUPED) {
+          if (tr.p != last_q) {
+            // the problem's tensor maps live in global memory that the host rewrites between
+            // launches: order those writes before the tensor-map reads of the loads
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tr.mA) : "memory");
+            asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tr.mB) : "memory");
+            last_q = tr.p;
+          }
+        }
+        const TileCoord tc = tile_coord(q, tr.t);
+        const int bpb = q.BN * KBLK;  // bytes of one B plane of this tile
+        const uint32_t tile_stage_bytes = (uint32_t)(S * (L.a_plane_bytes + bpb));
+        const int nkb = q.nkb;
+        const int64_t rowsA_pad = q.rowsA_pad, rowsB_pad = q.rowsB_pad;
+        for (int kb = 0; kb < nkb; ++kb, ++it) {
           const int st = (int)(it % L.stages);
           const uint32_t ph = (uint32_t)((it / L.stages) & 1);
           if (it >= L.stages && !mbar_wait(&empty_bar[st], ph ^ 1, abort_flag)) {
@@ -637,15 +689,15 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
             break;
           }
           uint8_t* sbase = tiles + (size_t)st * L.stage_bytes;
-          mbar_expect_tx(&full_bar[st], (uint32_t)L.stage_bytes);
+          mbar_expect_tx(&full_bar[st], tile_stage_bytes);
           for (int s = 0; s < S; ++s) {
-            const int ya = (int)((tc.rbA * S + s) * p.rowsA_pad + tc.mrow0);
-            tma_load_2d(sbase + s * L.a_plane_bytes, &mapA, kb * KBLK, ya, &full_bar[st]);
+            const int ya = (int)((tc.rbA * S + s) * rowsA_pad + tc.mrow0);
+            tma_load_2d(sbase + s * L.a_plane_bytes, tr.mA, kb * KBLK, ya, &full_bar[st]);
           }
           uint8_t* bbase = sbase + S * L.a_plane_bytes;
           for (int u = 0; u < S; ++u) {
-            const int yb = (int)((tc.rbB * S + u) * p.rowsB_pad + tc.ncol0);
-            tma_load_2d(bbase + u * L.b_plane_bytes, &mapB, kb * KBLK, yb, &full_bar[st]);
+            const int yb = (int)((tc.rbB * S + u) * rowsB_pad + tc.ncol0);
+            tma_load_2d(bbase + u * bpb, tr.mB, kb * KBLK, yb, &full_bar[st]);
           }
           issued = it + 1;
         }
@@ -653,9 +705,11 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const uint32_t idesc = idesc_i8(p.BN);
       int64_t it = 0, tcount = 0;
       for (int64_t t = blockIdx.x; t < ntiles && !*abort_flag; t += gridDim.x, ++tcount) {
+        const TileRef tr = tile_ref<GROUPED>(p, &mapA, &mapB, t);
+        const int tbn = tr.p->BN, nkb = tr.p->nkb;
+        const uint32_t idesc = idesc_i8(tbn);
         const int buf = (int)(tcount % nbuf);
         const int64_t use = tcount / nbuf;
         if (use > 0 && !mbar_wait(&acce_bar[buf], (uint32_t)((use - 1) & 1), abort_flag)) {
@@ -666,7 +720,7 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
         tc_fence_after();
         const uint32_t acc = tmem_base + (uint32_t)buf * acc_cols;
         bool ok = true;
-        for (int kb = 0; kb < p.nkb; ++kb, ++it) {
+        for (int kb = 0; kb < nkb; ++kb, ++it) {
           const int st = (int)(it % L.stages);
           const uint32_t ph = (uint32_t)((it / L.stages) & 1);
           if (!mbar_wait(&full_bar[st], ph, abort_flag)) {
@@ -681,8 +735,8 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
           for (int s = 0; s < S; ++s) {
             const uint64_t ad = smem_desc_sw64(smem_u32(sbase + s * L.a_plane_bytes));
             for (int u = 0; s + u < S; ++u) {
-              const uint64_t bd = smem_desc_sw64(smem_u32(bbase + u * L.b_plane_bytes));
-              const uint32_t dt = acc + (uint32_t)((s + u) * p.BN);
+              const uint64_t bd = smem_desc_sw64(smem_u32(bbase + u * tbn * KBLK));
+              const uint32_t dt = acc + (uint32_t)((s + u) * tbn);
 #pragma unroll
               for (int kk = 0; kk < KBLK / 32; ++kk)
                 umma_i8(dt, ad + 2 * kk, bd + 2 * kk, idesc, (kb > 0 || kk > 0 || s > 0) ? 1u : 0u);
@@ -709,24 +763,26 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
     constexpr int H = EPI_CG / 2;
     int64_t tcount = 0;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++tcount) {
-      const TileCoord tc = tile_coord(p, t);
+      const TileRef tr = tile_ref<GROUPED>(p, &mapA, &mapB, t);
+      const GemmParams& q = *tr.p;  // this tile's problem
+      const TileCoord tc = tile_coord(q, tr.t);
       const int buf = (int)(tcount % nbuf);
       const int64_t use = tcount / nbuf;
       uint8_t* tb = tables + (tcount & 1) * tsb;
       int64_t* sh_rowC = reinterpret_cast<int64_t*>(tb);
       int64_t* sh_colC = sh_rowC + TILE_M / 2;
-      double* sh_csc = reinterpret_cast<double*>(sh_colC + p.BN);  // column factors 2^(eb - 7(S+1))
-      int32_t* sh_eA = reinterpret_cast<int32_t*>(sh_csc + p.BN);
+      double* sh_csc = reinterpret_cast<double*>(sh_colC + q.BN);  // column factors 2^(eb - 7(S+1))
+      int32_t* sh_eA = reinterpret_cast<int32_t*>(sh_csc + q.BN);
       // (filled while the MMAs of this tile run)
-      for (int i = et; i < TILE_M / 2 + p.BN; i += EPI_THREADS) {
+      for (int i = et; i < TILE_M / 2 + q.BN; i += EPI_THREADS) {
         if (i < TILE_M / 2) {
           const int64_t m = tc.mrow0 / 2 + i;
-          sh_eA[i] = m < p.M ? p.eA[tc.rbA * p.eA_ld + m] : 0;
-          sh_rowC[i] = m < p.M ? p.C.row(m) : 0;
+          sh_eA[i] = m < q.M ? q.eA[tc.rbA * q.eA_ld + m] : 0;
+          sh_rowC[i] = m < q.M ? q.C.row(m) : 0;
         } else {
           const int64_t n = tc.ncol0 + (i - TILE_M / 2);
-          const int eb = n < p.N ? p.eB[tc.rbB * p.eB_ld + n] : 0;
-          sh_colC[i - TILE_M / 2] = n < p.N ? p.C.col(n) : 0;
+          const int eb = n < q.N ? q.eB[tc.rbB * q.eB_ld + n] : 0;
+          sh_colC[i - TILE_M / 2] = n < q.N ? q.C.col(n) : 0;
           sh_csc[i - TILE_M / 2] = pow2(eb - 7 * (S + 1));
         }
       }
@@ -744,28 +800,28 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
       tc_fence_after();
       // a real alpha that is a power of two is folded into the row factor (exact, so the result
       // equals the validation engine's alpha * value); the store is then a plain copy
-      const bool alpha_in_tile = p.alpha_pow2 != 0;
-      const double rs = alpha_in_tile ? pow2(sh_eA[mloc]) * p.alpha.x : pow2(sh_eA[mloc]);
+      const bool alpha_in_tile = q.alpha_pow2 != 0;
+      const double rs = alpha_in_tile ? pow2(sh_eA[mloc]) * q.alpha.x : pow2(sh_eA[mloc]);
       // a warp whose 32 rows are all padding skips the accumulator reads
-      const bool live = tc.mrow0 + sp * 32 < 2 * p.M;
+      const bool live = tc.mrow0 + sp * 32 < 2 * q.M;
       const uint32_t acc = tmem_base + (uint32_t)buf * acc_cols + ((uint32_t)(sp * 32) << 16);
-      const int64_t mlim = p.M - tc.mrow0 / 2, nlim = p.N - tc.ncol0;
+      const int64_t mlim = q.M - tc.mrow0 / 2, nlim = q.N - tc.ncol0;
       const bool mok = mloc < mlim;
-      cplx* Crow = p.C.ptr + p.C.bat(tc.b0, tc.b1, tc.b2) + sh_rowC[mloc];
-      const bool has_beta = p.beta.x != 0.0 || p.beta.y != 0.0;
-      for (int c0 = 0; c0 < p.BN; c0 += EPI_CH) {
-        const int cw = min(EPI_CH, p.BN - c0);
+      cplx* Crow = q.C.ptr + q.C.bat(tc.b0, tc.b1, tc.b2) + sh_rowC[mloc];
+      const bool has_beta = q.beta.x != 0.0 || q.beta.y != 0.0;
+      for (int c0 = 0; c0 < q.BN; c0 += EPI_CH) {
+        const int cw = min(EPI_CH, q.BN - c0);
         const int cc = grp * EPI_CG;
-        const bool last = c0 + EPI_CH >= p.BN;
+        const bool last = c0 + EPI_CH >= q.BN;
         double v[EPI_CG];
         const bool work = live && cc < cw;
         if (work) {
           // all S diagonals of the warp's 8 columns in one TMEM round trip
-          int32_t q[S][1][EPI_CG];
+          int32_t dq[S][1][EPI_CG];
 #pragma unroll
-          for (int d = 0; d < S; ++d) tmem_ld8(acc + (uint32_t)(d * p.BN + c0 + cc), q[d][0]);
+          for (int d = 0; d < S; ++d) tmem_ld8(acc + (uint32_t)(d * q.BN + c0 + cc), dq[d][0]);
           tmem_wait_ld();
-          combine_cols<S, EPI_CG>(q, p.pair != 0, v);
+          combine_cols<S, EPI_CG>(dq, q.pair != 0, v);
         }
         if (last) {
           // this warp's reads of the accumulator set are complete: release it to the MMA warp
@@ -787,8 +843,8 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
               if (col < nlim) {
                 cplx* d = Crow + sh_colC[col];
                 cplx val = r ? cmk(other[i], v[H + i]) : cmk(v[i], other[i]);
-                if (!alpha_in_tile) val = cmul(p.alpha, val);
-                if (has_beta) val = cadd(val, cmul(p.beta, *d));
+                if (!alpha_in_tile) val = cmul(q.alpha, val);
+                if (has_beta) val = cadd(val, cmul(q.beta, *d));
                 *d = val;
               }
             }
@@ -902,6 +958,7 @@ struct SplitEngine {
   DevArray<int8_t> planesA, planesB;
   DevArray<int32_t> expA, expB;
   DevArray<int> err;
+  DevArray<GroupEntry> group;  // problems of a grouped launch (tensor maps, parameters, tile ranges)
   bool attr_set = false;
 };
 
@@ -967,22 +1024,37 @@ void run_slicer(SliceJob& j, int64_t nrb, cudaStream_t st) {
 
 }  // namespace
 
-void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st, int slices) {
-  if (g0.M <= 0 || g0.N <= 0) return;
-  validate(g0);
-  const int S = slices > 0 ? slices : c.slices;
-  require(S >= 2 && S <= 8, GB200_ERR_INVALID, "split: slices out of range");
-  require(g0.K > 0, GB200_ERR_INVALID, "split: empty contraction");
-  // One TMEM accumulator set of up to 512 columns and the widest tile it allows.  Measured on
-  // B200 for every launch shape of the GW chain, this is faster than two sets of half the width
-  // (the epilogue of one tile overlapping the next tile's MMAs), with one MMA per slice product
-  // or with one MMA of width (S - s) BN per A slice plane: narrower tiles double the per-tile
-  // epilogue work (tables, barrier, TMEM round trips) that dominates the short contractions.
-  const int nbuf = 1;
-  const int BN = std::min<int>(max_bn(S, 512 / nbuf), (int)rup(g0.N, 16));
-  // largest K chunk for which no INT32 diagonal can overflow: S * 2K * 127^2 < 2^31
+namespace {
+
+// largest K chunk for which no INT32 diagonal can overflow: S * 2K * 127^2 < 2^31
+int64_t kmax_for(int S) {
   int64_t kmax = (int64_t)(2147483647.0 / (2.0 * 127.0 * 127.0 * S));
-  kmax = kmax / 32 * 32;
+  return kmax / 32 * 32;
+}
+
+// Tile width of a problem: one TMEM accumulator set of up to 512 columns and the widest tile it
+// allows, or the context's chosen width.  Measured on B200 for every launch shape of the GW
+// chain, one set of the widest tile is faster than two sets of half the width (the epilogue of
+// one tile overlapping the next tile's MMAs), with one MMA per slice product or with one MMA of
+// width (S - s) BN per A slice plane: narrower tiles double the per-tile epilogue work (tables,
+// barrier, TMEM round trips) that dominates the short contractions.
+int tile_width(const Context& c, int S, int64_t N) {
+  int bn = max_bn(S, 512);
+  if (c.tile_bn > 0) bn = std::min(bn, std::max(16, c.tile_bn / 16 * 16));
+  return std::min<int>(bn, (int)rup(N, 16));
+}
+
+struct Prepared {
+  GemmParams p{};
+  CUtensorMap mA{}, mB{};
+  int64_t kpad = 0, ntiles = 0;
+  double flops = 0.0;
+};
+
+// Slice K chunk [k0, k0 + Kc) of both operands into the engine's planes and fill the problem's
+// parameters (and, for the tensor-core engine, its tensor maps).
+Prepared prepare_chunk(SplitEngine& se, const ZGemm& g0, int S, int BN, int64_t k0, int64_t Kc, cudaStream_t st) {
+  Prepared pr;
   int depA[3], depB[3];
   deps_of(g0.A, depA);
   deps_of(g0.B, depB);
@@ -993,119 +1065,225 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st, i
     se.err.alloc(1);
     GB_CUDA(cudaMemsetAsync(se.err.p, 0, sizeof(int), st));
   }
+  const int64_t kpad = rup(2 * Kc, KBLK);
+  se.planesA.alloc((size_t)(nrbA * S * rowsA_pad * kpad));
+  se.planesB.alloc((size_t)(nrbB * S * rowsB_pad * kpad));
+  se.expA.alloc((size_t)(nrbA * rowsA_pad / 2));
+  se.expB.alloc((size_t)(nrbB * rowsB_pad));
+  {
+    SliceJob j{};
+    j.ptr = g0.A.ptr; j.rmap = g0.A.row; j.kmap = g0.A.col; j.bat = g0.A.bat; j.conj = g0.A.conj;
+    j.R = g0.M; j.K = Kc; j.k0 = k0; j.n0 = g0.nb0; j.n1 = g0.nb1; j.n2 = g0.nb2;
+    std::copy(depA, depA + 3, j.dep);
+    j.embed = 1; j.S = S; j.rows_pad = rowsA_pad; j.rpad = rowsA_pad / 2; j.kpad = kpad; j.e_ld = rowsA_pad / 2;
+    j.out = se.planesA.p; j.expo = se.expA.p;
+    j.r_fast = std::abs(g0.A.row.s_in) < std::abs(g0.A.col.s_in);
+    run_slicer(j, nrbA, st);
+  }
+  {
+    SliceJob j{};
+    // right operand sliced per column: the job's rows are the N columns, K runs along B's rows
+    j.ptr = g0.B.ptr; j.rmap = g0.B.col; j.kmap = g0.B.row; j.bat = g0.B.bat; j.conj = g0.B.conj;
+    j.R = g0.N; j.K = Kc; j.k0 = k0; j.n0 = g0.nb0; j.n1 = g0.nb1; j.n2 = g0.nb2;
+    std::copy(depB, depB + 3, j.dep);
+    j.embed = 0; j.S = S; j.rows_pad = rowsB_pad; j.rpad = rowsB_pad; j.kpad = kpad; j.e_ld = rowsB_pad;
+    j.out = se.planesB.p; j.expo = se.expB.p;
+    j.r_fast = std::abs(g0.B.col.s_in) < std::abs(g0.B.row.s_in);
+    run_slicer(j, nrbB, st);
+  }
+  GemmParams& p = pr.p;
+  p.S = S; p.BN = BN; p.nkb = (int)(kpad / KBLK);
+  p.M = g0.M; p.N = g0.N; p.nb0 = g0.nb0; p.nb1 = g0.nb1; p.nb2 = g0.nb2;
+  std::copy(depA, depA + 3, p.depA);
+  std::copy(depB, depB + 3, p.depB);
+  p.rowsA_pad = rowsA_pad; p.rowsB_pad = rowsB_pad;
+  p.eA = se.expA.p; p.eB = se.expB.p; p.eA_ld = rowsA_pad / 2; p.eB_ld = rowsB_pad;
+  p.C = g0.C; p.alpha = g0.alpha; p.beta = (k0 == 0) ? g0.beta : cmk(1.0, 0.0);
+  p.err = se.err.p;
+  {
+    int aexp = 0;
+    p.alpha_pow2 = (g0.alpha.y == 0.0 && g0.alpha.x != 0.0 && std::fabs(std::frexp(g0.alpha.x, &aexp)) == 0.5) ? 1 : 0;
+  }
+  {
+    // |q_d| <= (d + 1) * 2Kc * 64^2 (d + 1 digit pairs per diagonal, balanced digits |q| <= 64):
+    // pair (d, d + 1) is exact in int32 when 128 max|q_d| + max|q_(d+1)| < 2^31
+    bool ok = S <= 5;
+    for (int d = 0; ok && d + 1 < S && d <= 2; d += 2)
+      ok = 2.0 * (double)Kc * 4096.0 * (128.0 * (d + 1) + (d + 2)) < 2147483648.0;
+    p.pair = ok ? 1 : 0;
+  }
+  p.rows_fast = std::abs(g0.C.row.s_in) < std::abs(g0.C.col.s_in) ? 1 : 0;
+  const int64_t nbatch = g0.nb0 * g0.nb1 * g0.nb2;
+  require(nbatch < 65536, GB200_ERR_INVALID, "split: too many batches for one launch");
+  p.tiles_m = (int)(rowsA_pad / TILE_M);
+  p.tiles_n = (int)(rowsB_pad / BN);
+  pr.kpad = kpad;
+  pr.ntiles = (int64_t)p.tiles_m * p.tiles_n * nbatch;
+  pr.flops = 8.0 * (double)g0.M * (double)g0.N * (double)Kc * (double)nbatch;
+  if (se.core == 0) {
+    const int64_t rowsA_total = nrbA * S * rowsA_pad;
+    const int64_t rowsB_total = nrbB * S * rowsB_pad;
+    require(rowsA_total < (1LL << 31) && rowsB_total < (1LL << 31), GB200_ERR_INVALID, "split: operand too large for TMA");
+    pr.mA = make_map(se.planesA.p, kpad, rowsA_total, TILE_M);
+    pr.mB = make_map(se.planesB.p, kpad, rowsB_total, BN);
+  }
+  return pr;
+}
+
+template <bool G>
+void set_smem_attrs() {
+  const void* fns[] = {(const void*)split_gemm_tc_kernel<2, G>, (const void*)split_gemm_tc_kernel<3, G>,
+                       (const void*)split_gemm_tc_kernel<4, G>, (const void*)split_gemm_tc_kernel<5, G>,
+                       (const void*)split_gemm_tc_kernel<6, G>, (const void*)split_gemm_tc_kernel<7, G>,
+                       (const void*)split_gemm_tc_kernel<8, G>};
+  for (const void* f : fns) GB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+}
+
+template <bool G>
+void launch_tc(int S, unsigned grid, size_t smem, cudaStream_t st, const CUtensorMap& mA, const CUtensorMap& mB,
+               const GemmParams& p) {
+  switch (S) {
+    case 2: split_gemm_tc_kernel<2, G><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+    case 3: split_gemm_tc_kernel<3, G><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+    case 4: split_gemm_tc_kernel<4, G><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+    case 5: split_gemm_tc_kernel<5, G><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+    case 6: split_gemm_tc_kernel<6, G><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+    case 7: split_gemm_tc_kernel<7, G><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+    default: split_gemm_tc_kernel<8, G><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+  }
+  GB_CHECK_LAUNCH();
+}
+
+// Launch-wide layout for tiles up to BN columns: TMA ring depth (what fits, at most 6 K blocks)
+// and the dynamic shared memory.
+void ring_layout(int S, int BN, GemmParams& p, size_t& smem) {
+  const SmemLayout L1 = smem_layout(S, BN, 1);
+  int stages = (SMEM_BUDGET - L1.ctile_bytes - 4096) / L1.stage_bytes;
+  stages = std::max(1, std::min(stages, 6));
+  p.stages = stages;
+  p.nbuf = 1;
+  const SmemLayout Ls = smem_layout(S, BN, stages);
+  smem = (size_t)Ls.ring_bytes + Ls.ctile_bytes + 1024 /*alignment*/ + misc_bytes(stages, BN);
+  require(smem <= 227 * 1024, GB200_ERR_INVALID, "split: shared memory budget exceeded");
+}
+
+KernelRecord* begin_record(Context& c, double flops, cudaStream_t st) {
+  if (!c.stats_on) return nullptr;
+  if (c.records_used == c.records.size()) {
+    KernelRecord r;
+    GB_CUDA(cudaEventCreate(&r.start));
+    GB_CUDA(cudaEventCreate(&r.stop));
+    c.records.push_back(r);
+  }
+  KernelRecord* rec = &c.records[c.records_used++];
+  rec->alg_flops = flops;  // FP64-equivalent work: 8 real flops per complex multiply-add
+  GB_CUDA(cudaEventRecord(rec->start, st));
+  return rec;
+}
+
+unsigned persistent_grid(const Context& c, int64_t ntiles) {
+  require(ntiles < (1LL << 31), GB200_ERR_INVALID, "split: too many tiles for one launch");
+  int nsm = 148;
+  GB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.device));
+  return (unsigned)std::min<int64_t>(ntiles, nsm);  // one CTA per SM walks the tiles
+}
+
+}  // namespace
+
+void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st, int slices) {
+  if (g0.M <= 0 || g0.N <= 0) return;
+  validate(g0);
+  const int S = slices > 0 ? slices : c.slices;
+  require(S >= 2 && S <= 8, GB200_ERR_INVALID, "split: slices out of range");
+  require(g0.K > 0, GB200_ERR_INVALID, "split: empty contraction");
+  const int BN = tile_width(c, S, g0.N);
+  const int64_t kmax = kmax_for(S);
   for (int64_t k0 = 0; k0 < g0.K; k0 += kmax) {
     const int64_t Kc = std::min(kmax, g0.K - k0);
-    const int64_t kpad = rup(2 * Kc, KBLK);
-    se.planesA.alloc((size_t)(nrbA * S * rowsA_pad * kpad));
-    se.planesB.alloc((size_t)(nrbB * S * rowsB_pad * kpad));
-    se.expA.alloc((size_t)(nrbA * rowsA_pad / 2));
-    se.expB.alloc((size_t)(nrbB * rowsB_pad));
-    {
-      SliceJob j{};
-      j.ptr = g0.A.ptr; j.rmap = g0.A.row; j.kmap = g0.A.col; j.bat = g0.A.bat; j.conj = g0.A.conj;
-      j.R = g0.M; j.K = Kc; j.k0 = k0; j.n0 = g0.nb0; j.n1 = g0.nb1; j.n2 = g0.nb2;
-      std::copy(depA, depA + 3, j.dep);
-      j.embed = 1; j.S = S; j.rows_pad = rowsA_pad; j.rpad = rowsA_pad / 2; j.kpad = kpad; j.e_ld = rowsA_pad / 2;
-      j.out = se.planesA.p; j.expo = se.expA.p;
-      j.r_fast = std::abs(g0.A.row.s_in) < std::abs(g0.A.col.s_in);
-      run_slicer(j, nrbA, st);
-    }
-    {
-      SliceJob j{};
-      // right operand sliced per column: the job's rows are the N columns, K runs along B's rows
-      j.ptr = g0.B.ptr; j.rmap = g0.B.col; j.kmap = g0.B.row; j.bat = g0.B.bat; j.conj = g0.B.conj;
-      j.R = g0.N; j.K = Kc; j.k0 = k0; j.n0 = g0.nb0; j.n1 = g0.nb1; j.n2 = g0.nb2;
-      std::copy(depB, depB + 3, j.dep);
-      j.embed = 0; j.S = S; j.rows_pad = rowsB_pad; j.rpad = rowsB_pad; j.kpad = kpad; j.e_ld = rowsB_pad;
-      j.out = se.planesB.p; j.expo = se.expB.p;
-      j.r_fast = std::abs(g0.B.col.s_in) < std::abs(g0.B.row.s_in);
-      run_slicer(j, nrbB, st);
-    }
-    GemmParams p{};
-    p.S = S; p.BN = BN; p.nkb = (int)(kpad / KBLK);
-    p.M = g0.M; p.N = g0.N; p.nb0 = g0.nb0; p.nb1 = g0.nb1; p.nb2 = g0.nb2;
-    std::copy(depA, depA + 3, p.depA);
-    std::copy(depB, depB + 3, p.depB);
-    p.rowsA_pad = rowsA_pad; p.rowsB_pad = rowsB_pad;
-    p.eA = se.expA.p; p.eB = se.expB.p; p.eA_ld = rowsA_pad / 2; p.eB_ld = rowsB_pad;
-    p.C = g0.C; p.alpha = g0.alpha; p.beta = (k0 == 0) ? g0.beta : cmk(1.0, 0.0);
-    p.err = se.err.p;
-    {
-      int aexp = 0;
-      p.alpha_pow2 = (g0.alpha.y == 0.0 && g0.alpha.x != 0.0 && std::fabs(std::frexp(g0.alpha.x, &aexp)) == 0.5) ? 1 : 0;
-    }
-    {
-      // |q_d| <= (d + 1) * 2Kc * 64^2 (d + 1 digit pairs per diagonal, balanced digits |q| <= 64):
-      // pair (d, d + 1) is exact in int32 when 128 max|q_d| + max|q_(d+1)| < 2^31
-      bool ok = S <= 5;
-      for (int d = 0; ok && d + 1 < S && d <= 2; d += 2)
-        ok = 2.0 * (double)Kc * 4096.0 * (128.0 * (d + 1) + (d + 2)) < 2147483648.0;
-      p.pair = ok ? 1 : 0;
-    }
-    p.rows_fast = std::abs(g0.C.row.s_in) < std::abs(g0.C.col.s_in) ? 1 : 0;
+    Prepared pr = prepare_chunk(se, g0, S, BN, k0, Kc, st);
     const int64_t nbatch = g0.nb0 * g0.nb1 * g0.nb2;
-    require(nbatch < 65536, GB200_ERR_INVALID, "split: too many batches for one launch");
     if (se.core == 1) {
       dim3 grid((unsigned)((g0.N + 15) / 16), (unsigned)((g0.M + 15) / 16), (unsigned)nbatch);
-      split_gemm_ref_kernel<<<grid, dim3(16, 16), 0, st>>>(se.planesA.p, se.planesB.p, kpad, p);
+      split_gemm_ref_kernel<<<grid, dim3(16, 16), 0, st>>>(se.planesA.p, se.planesB.p, pr.kpad, pr.p);
       GB_CHECK_LAUNCH();
-    } else {
-      const int64_t rowsA_total = nrbA * S * rowsA_pad;
-      const int64_t rowsB_total = nrbB * S * rowsB_pad;
-      require(rowsA_total < (1LL << 31) && rowsB_total < (1LL << 31), GB200_ERR_INVALID, "split: operand too large for TMA");
-      CUtensorMap mA = make_map(se.planesA.p, kpad, rowsA_total, TILE_M);
-      CUtensorMap mB = make_map(se.planesB.p, kpad, rowsB_total, BN);
-      // TMA ring depth: what fits next to the result tile, at most 6 K blocks
-      const SmemLayout L1 = smem_layout(S, BN, 1);
-      int stages = (SMEM_BUDGET - L1.ctile_bytes - 4096) / L1.stage_bytes;
-      stages = std::max(1, std::min(stages, 6));
-      p.stages = stages;
-      p.nbuf = nbuf;
-      p.tiles_m = (int)(rowsA_pad / TILE_M);
-      p.tiles_n = (int)(rowsB_pad / BN);
-      const SmemLayout Ls = smem_layout(S, BN, stages);
-      const size_t smem = (size_t)Ls.ring_bytes + Ls.ctile_bytes + 1024 /*alignment*/ + misc_bytes(stages, BN);
-      if (!se.attr_set) {
-        const void* fns[] = {(const void*)split_gemm_tc_kernel<2>, (const void*)split_gemm_tc_kernel<3>,
-                             (const void*)split_gemm_tc_kernel<4>, (const void*)split_gemm_tc_kernel<5>,
-                             (const void*)split_gemm_tc_kernel<6>, (const void*)split_gemm_tc_kernel<7>,
-                             (const void*)split_gemm_tc_kernel<8>};
-        for (const void* f : fns)
-          GB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-        se.attr_set = true;
-      }
-      require(smem <= 227 * 1024, GB200_ERR_INVALID, "split: shared memory budget exceeded");
-      // persistent launch: one CTA per SM walks the tiles
-      const int64_t ntiles = (int64_t)p.tiles_m * p.tiles_n * nbatch;
-      require(ntiles < (1LL << 31), GB200_ERR_INVALID, "split: too many tiles for one launch");
-      int nsm = 148;
-      GB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c.device));
-      const unsigned grid = (unsigned)std::min<int64_t>(ntiles, nsm);
-      KernelRecord* rec = nullptr;
-      if (c.stats_on) {
-        if (c.records_used == c.records.size()) {
-          KernelRecord r;
-          GB_CUDA(cudaEventCreate(&r.start));
-          GB_CUDA(cudaEventCreate(&r.stop));
-          c.records.push_back(r);
-        }
-        rec = &c.records[c.records_used++];
-        // FP64-equivalent work of this K chunk: 8 real flops per complex multiply-add
-        rec->alg_flops = 8.0 * (double)g0.M * (double)g0.N * (double)Kc * (double)nbatch;
-        GB_CUDA(cudaEventRecord(rec->start, st));
-      }
-      switch (S) {
-        case 2: split_gemm_tc_kernel<2><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
-        case 3: split_gemm_tc_kernel<3><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
-        case 4: split_gemm_tc_kernel<4><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
-        case 5: split_gemm_tc_kernel<5><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
-        case 6: split_gemm_tc_kernel<6><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
-        case 7: split_gemm_tc_kernel<7><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
-        default: split_gemm_tc_kernel<8><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
-      }
-      GB_CHECK_LAUNCH();
-      if (rec) GB_CUDA(cudaEventRecord(rec->stop, st));
+      continue;
     }
+    size_t smem = 0;
+    ring_layout(S, BN, pr.p, smem);
+    if (!se.attr_set) {
+      set_smem_attrs<false>();
+      set_smem_attrs<true>();
+      se.attr_set = true;
+    }
+    KernelRecord* rec = begin_record(c, pr.flops, st);
+    launch_tc<false>(S, persistent_grid(c, pr.ntiles), smem, st, pr.mA, pr.mB, pr.p);
+    if (rec) GB_CUDA(cudaEventRecord(rec->stop, st));
+  }
+}
+
+void split_gemm_group(const std::vector<Context*>& cs, const std::vector<ZGemm>& gs, cudaStream_t st, int slices) {
+  require(cs.size() == gs.size() && !cs.empty(), GB200_ERR_INVALID, "split group: one contraction per context");
+  const int S = slices;
+  require(S >= 2 && S <= 8, GB200_ERR_INVALID, "split: slices out of range");
+  const int64_t kmax = kmax_for(S);
+  std::vector<SplitEngine*> ses;
+  std::vector<int> bns;
+  int64_t nch = 0;
+  bool tc_engine = true;
+  for (size_t i = 0; i < cs.size(); ++i) {
+    for (size_t j = 0; j < i; ++j)
+      require(cs[j] != cs[i], GB200_ERR_INVALID, "split group: a context appears twice (its slice buffers are shared)");
+    validate(gs[i]);
+    require(gs[i].K > 0 && gs[i].M > 0 && gs[i].N > 0, GB200_ERR_INVALID, "split group: empty contraction");
+    ses.push_back(split_engine(*cs[i]));
+    tc_engine = tc_engine && ses.back()->core == 0;
+    bns.push_back(tile_width(*cs[i], S, gs[i].N));
+    nch = std::max<int64_t>(nch, (gs[i].K + kmax - 1) / kmax);
+  }
+  if (!tc_engine) {  // the CUDA-core validation engine has no grouped form
+    for (size_t i = 0; i < cs.size(); ++i) split_gemm(*cs[i], *ses[i], gs[i], st, S);
+    return;
+  }
+  SplitEngine& se0 = *ses[0];
+  if (!se0.attr_set) {
+    set_smem_attrs<false>();
+    set_smem_attrs<true>();
+    se0.attr_set = true;
+  }
+  // K chunk ch of every problem that has one, all in one grouped launch per chunk
+  for (int64_t ch = 0; ch < nch; ++ch) {
+    std::vector<GroupEntry> entries;
+    int BNmax = 16;
+    double flops = 0.0;
+    int64_t total = 0;
+    for (size_t i = 0; i < cs.size(); ++i) {
+      const int64_t k0 = ch * kmax;
+      if (k0 >= gs[i].K) continue;
+      Prepared pr = prepare_chunk(*ses[i], gs[i], S, bns[i], k0, std::min(kmax, gs[i].K - k0), st);
+      GroupEntry e;
+      e.mA = pr.mA;
+      e.mB = pr.mB;
+      e.p = pr.p;
+      e.tile_begin = total;
+      entries.push_back(e);
+      total += pr.ntiles;
+      BNmax = std::max(BNmax, bns[i]);
+      flops += pr.flops;
+    }
+    GemmParams p{};
+    p.S = S;
+    p.BN = BNmax;
+    p.err = se0.err.p;
+    size_t smem = 0;
+    ring_layout(S, BNmax, p, smem);
+    se0.group.alloc(entries.size());
+    GB_CUDA(cudaMemcpyAsync(se0.group.p, entries.data(), entries.size() * sizeof(GroupEntry), cudaMemcpyHostToDevice, st));
+    p.group = se0.group.p;
+    p.ngroup = (int)entries.size();
+    p.ntiles = total;
+    KernelRecord* rec = begin_record(*cs[0], flops, st);
+    launch_tc<true>(S, persistent_grid(*cs[0], total), smem, st, entries[0].mA, entries[0].mB, p);
+    if (rec) GB_CUDA(cudaEventRecord(rec->stop, st));
   }
 }
 

@@ -1,6 +1,8 @@
 // Split-precision (Ozaki-sliced INT8 tensor-core) contractions.
 #pragma once
 
+#include <vector>
+
 #include "context.cuh"
 
 namespace gb200 {
@@ -13,6 +15,10 @@ SplitEngine* split_engine(Context& c);
 // products on the tensor cores with exact INT32 accumulation, FP64 recombination;
 // `slices` pieces per operand (0: the context's count).
 void split_gemm(Context& c, SplitEngine& se, const ZGemm& g, cudaStream_t st, int slices = 0);
+// The same for one contraction of each of several contexts (distinct contexts, all in split
+// precision with `slices` pieces): every context slices its operands into its own buffers and one
+// persistent tensor-core launch per K chunk walks the tiles of all of them.
+void split_gemm_group(const std::vector<Context*>& cs, const std::vector<ZGemm>& gs, cudaStream_t st, int slices);
 void split_release(Context& c);
 // Non-zero if a split kernel hit a bounded-wait timeout since the last check (flag is cleared).
 int split_check_error(Context& c, cudaStream_t st);

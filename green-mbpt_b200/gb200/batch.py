@@ -1,7 +1,10 @@
 """Many independent systems on one GPU (the batched uneven-systems workload).
 
 Each system keeps its own context: its integrals, grid, maps and scratch buffers, and its own
-CUDA stream.  `run_gw` issues the self-energy of every system from a pool of host threads.  The
+CUDA stream.  `run_gw_grouped` evaluates all of them in one library call whose contraction stages
+are grouped persistent launches over the tiles of every system (gb200_gw_sigma_batch_device), with
+tile widths from the autotuner's table (`apply_tiles`).  `run_gw` instead issues the self-energy of
+every system from a pool of host threads.  The
 library calls release the interpreter lock, so the systems' kernels are queued on different
 streams and overlap on the device wherever one system does not fill it: the slicing and FP64
 kernels of one system run beside the contraction kernel of another.  Results are identical to
@@ -54,6 +57,26 @@ class SystemBatch:
 
         with cf.ThreadPoolExecutor(max_workers=self.workers) as ex:
             return list(ex.map(one, range(len(self))))
+
+    def run_gw_grouped(self, G_ptrs, Sigma_ptrs, stream: int = 0):
+        """gb200_gw_sigma_batch_device over all systems in one call: the systems' q-points in step,
+        each contraction stage one grouped persistent tensor-core launch over the tiles of every
+        system (all in split precision with the same slice count)."""
+        from . import lib
+        if len(G_ptrs) != len(self) or len(Sigma_ptrs) != len(self):
+            raise ValueError("one G and one Sigma buffer per system")
+        lib.gw_sigma_batch_device(self.contexts, G_ptrs, Sigma_ptrs, stream)
+
+    def apply_tiles(self, table=None):
+        """Tile width of every context from the autotuner's table (gb200.tune.choose_tile)."""
+        from . import tune
+        widths = []
+        for c in self.contexts:
+            d = c.dims
+            bn = tune.choose_tile(d.nao, d.NQ, table)
+            c.set_tile_width(bn)
+            widths.append(bn)
+        return widths
 
     def run_gw_host(self, Gs):
         """gw_sigma (host arrays in and out) for every system, concurrently."""

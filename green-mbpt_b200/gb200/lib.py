@@ -62,6 +62,7 @@ EXPORTED = [
     "gb200_set_q_range", "gb200_dyson_solve_device", "gb200_energy_device", "gb200_stats_enable", "gb200_stats_read",
     "gb200_hf_fock_noalloc", "gb200_set_q0_correction", "gb200_gw_sigma_vjp", "gb200_gw_sigma_vjp_device",
     "gb200_set_contraction_slices", "gb200_set_memory_budget", "gb200_set_integrals_pairs",
+    "gb200_gw_sigma_batch_device", "gb200_set_tile_width",
 ]
 
 
@@ -121,6 +122,8 @@ def load(path: str | None = None):
     L.gb200_hf_fock_noalloc.argtypes = [ctypes.POINTER(Dims), vp, vp, vp, ctypes.c_double, vp, vp]
     L.gb200_set_q0_correction.argtypes = [vp, vp, vp, ctypes.c_double]
     L.gb200_set_integrals_pairs.argtypes = [vp, vp, vp, ctypes.c_int64, ip, vp]
+    L.gb200_gw_sigma_batch_device.argtypes = [vp, ip, vp, vp, vp]
+    L.gb200_set_tile_width.argtypes = [vp, ip]
     _lib = L
     return L
 
@@ -302,6 +305,10 @@ class Context:
         self._check(self._L.gb200_set_integrals_device(self._h, which, ctypes.c_void_p(V_ptr), pair_begin, pair_count,
                                                        ctypes.c_void_p(stream)))
 
+    def set_tile_width(self, bn: int = 0):
+        """Column tile of the split-precision contractions (0: the widest that fits)."""
+        self._check(self._L.gb200_set_tile_width(self._h, int(bn)))
+
     def set_integrals_pairs(self, V_pairs, pair_ids, stream: int = 0):
         """q-sharded GW integrals: the stored pairs `pair_ids` (increasing half-storage indices,
         gb200.shard.pairs_for_q_range) with their blocks V_pairs [len, NQ, nao, nao]: a host
@@ -392,3 +399,17 @@ def check_integral_version(v: str):
     if rc != OK:
         raise ValueError("Version string format is incorrect. Expected format: major.minor.patch[suffix]")
     return True
+
+
+def gw_sigma_batch_device(contexts, G_ptrs, Sigma_ptrs, stream: int = 0):
+    """gb200_gw_sigma_batch_device: the self-energies of several contexts (device buffers) in one
+    call, every contraction stage one grouped tensor-core launch over all systems."""
+    n = len(contexts)
+    if len(G_ptrs) != n or len(Sigma_ptrs) != n or n == 0:
+        raise ValueError("one G and one Sigma buffer per context")
+    L = load()
+    hs = (ctypes.c_void_p * n)(*[c._h for c in contexts])
+    gs = (ctypes.c_void_p * n)(*G_ptrs)
+    ss = (ctypes.c_void_p * n)(*Sigma_ptrs)
+    rc = L.gb200_gw_sigma_batch_device(hs, n, gs, ss, ctypes.c_void_p(stream))
+    contexts[0]._check(rc)

@@ -101,6 +101,21 @@ int gb200_set_integrals_device(gb200_context* ctx, int which, const double* V_de
  * (the allreduce of :53-54).  Default: all q. */
 int gb200_set_q_range(gb200_context* ctx, int q_begin, int q_end);
 
+/* The self-energies of n contexts (independent systems of any shapes, one device) in one call:
+ * G_dev[i] and Sigma_dev[i] are device buffers of context i, as for gb200_gw_sigma_device.  The
+ * systems' q-points run in step (round r takes the r-th q-point of every system that has one, the
+ * k-blocks in step), and each contraction stage of a round is one grouped persistent tensor-core
+ * launch over the tiles of all systems when all of them use split precision with the same slice
+ * count.  Every system's result is the one gb200_gw_sigma_device gives it alone.  Errors are
+ * reported on ctxs[0]. */
+int gb200_gw_sigma_batch_device(gb200_context* const* ctxs, int n, const double* const* G_dev,
+                                double* const* Sigma_dev, void* stream);
+
+/* Column tile width of the split-precision contractions of a context (a multiple of 16, at most
+ * the widest tile that S slices allow; 0: the widest).  The batched workload's autotuner picks it
+ * per (nao, naux). */
+int gb200_set_tile_width(gb200_context* ctx, int bn);
+
 /* q-sharded storage of the GW integrals: only the stored pairs `pair_ids` (indices
  * k1*(k1+1)/2 + k2 with k1 >= k2, strictly increasing; `count` of them) with their blocks
  * V_pairs [count, NQ, nao, nao] in that order, host memory (on_device = 0) or device memory

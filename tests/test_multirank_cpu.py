@@ -178,3 +178,16 @@ def test_batch_memory_shares_are_proportional():
     sizes = [80 * 1 * 40 * 64, 80 * 1 * 240 * 48 * 48, 80 * 2 * 100 * 400]
     for c, x in zip(ctxs, sizes):
         assert abs(c.budget / 60e9 - x / sum(sizes)) < 1e-12
+
+
+def test_tile_table_lookup():
+    """The autotuner's table is read by nearest measured (nao, naux); without one the widest tile."""
+    from gb200 import tune
+    table = {"8x32": {"bn": 32}, "40x200": {"bn": 80}, "48x288": {"bn": 96}}
+    assert tune.choose_tile(9, 36, table) == 32
+    assert tune.choose_tile(40, 210, table) == 80
+    assert tune.choose_tile(47, 280, table) == 96
+    assert tune.choose_tile(20, 100, {}) == 0
+    for key, entry in tune.load_table().items():
+        nao, naux = (int(x) for x in key.split("x"))
+        assert entry["bn"] in tune.CANDIDATES and min(entry["ms"], key=lambda k: entry["ms"][k]) == str(entry["bn"])

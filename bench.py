@@ -41,10 +41,11 @@ import numpy as np  # noqa: E402
 
 METRIC = "GW iterations/s at nk=125,nao=40: split-prec vs FP64 on B200, max|ΔΣ|≤1e-8"
 # DRAM bytes (read + write) per FP64-equivalent flop of the tensor-core contraction kernel, from
-# one ncu capture of its six launch shapes on the c2-shaped profiling case (c2k2): 8.18 GB for
-# 3.80e11 flops.  Each shape's traffic scales with its k-point batch as its flops do, so the
-# roofline traffic per launch is this ratio times the step's flops per launch.
-TC_DRAM_BYTES_PER_FLOP = 8.18e9 / 3.80e11
+# one ncu capture of its six launch shapes on the c2-shaped profiling case (c2k2) with the current
+# kernel (profiles/split_gemm_tc_c2k2.md): 8.25 GB for 3.80e11 flops.  Each shape's traffic scales
+# with its k-point batch as its flops do, so the roofline traffic per launch is this ratio times
+# the step's flops per launch.
+TC_DRAM_BYTES_PER_FLOP = 8.25e9 / 3.80e11
 UNIT = "iterations/s"
 WORKLOADS = {
     "c2": "c2: nk=125 (5x5x5), nao=40, naux=250, ns=1, ntau=120, nw=120, beta=200, eps~U[-5,5]",

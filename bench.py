@@ -517,6 +517,8 @@ def main_gw_profile(args):
     if args.profile_fp64:
         from gb200 import lib
         ctx.set_precision(lib.PREC_FP64, args.slices)
+    if args.tile_width:
+        ctx.set_tile_width(args.tile_width)
     G = torch.from_numpy(s.G).cuda()
     Sig = torch.empty_like(G)
     ctx.set_q_range(0, min(args.gw_q, s.nk))
@@ -725,6 +727,8 @@ def parse(argv=None):
                     help="profiling case: time only the GW self-energy over q-points [0, GW_Q)")
     ap.add_argument("--profile-fp64", dest="profile_fp64", action="store_true",
                     help="profiling case in FP64 instead of split precision")
+    ap.add_argument("--tile-width", dest="tile_width", type=int, default=0,
+                    help="profiling case: column tile of the tensor-core contractions (0: the default)")
     ap.add_argument("--newton", type=int, default=0,
                     help="differentiable-step case (--config c4): adjoint timings, then N plain and N "
                          "Newton-Krylov self-consistency steps from the same start")

@@ -430,53 +430,85 @@ __global__ void __launch_bounds__(SL_NT, 4) slice_write_kernel(SliceJob j) {
   write_digits(j, vals, rb, r, k, e);
 }
 
-// Both passes in one block for contractions of moderate length: a block owns TR rows over the
-// whole contraction range, finds their exponents, then reads the rows again (from L2) and writes
-// the slices.  The operand makes one trip from HBM instead of two.
-__global__ void __launch_bounds__(SL_NT, 3) slice_fused_kernel(SliceJob j, int nkt) {
-  __shared__ cplx tile[TR][TKP];
-  __shared__ int64_t roff[TR], koff[TK];
-  __shared__ double rmax[TR];
-  const int64_t rb = blockIdx.z, r0 = (int64_t)blockIdx.x * TR;
+// One pass for contractions of moderate length (K up to 8 tiles): a block stages RB rows over the
+// whole contraction range in shared memory, reduces their exponents there and writes the slices,
+// so the operand is read from HBM once.  Row layout in shared memory as in the tile kernels (one
+// spare slot after every 8 complex values: the 8 threads reading consecutive groups of a row hit
+// different banks).
+__host__ __device__ inline int resident_ld(int kt) { return kt + kt / 8 + 1; }
+
+inline size_t resident_smem(int rb, int kt) {
+  return (size_t)rb * resident_ld(kt) * sizeof(cplx) + (size_t)(rb + kt) * sizeof(int64_t) + rb * sizeof(double);
+}
+
+template <int RB>
+__global__ void __launch_bounds__(SL_NT) slice_resident_kernel(SliceJob j, int kt) {
+  extern __shared__ __align__(16) uint8_t sl_smem[];
+  const int ld = resident_ld(kt);
+  cplx* rows = reinterpret_cast<cplx*>(sl_smem);
+  int64_t* roff = reinterpret_cast<int64_t*>(rows + RB * ld);
+  int64_t* koff = roff + RB;
+  double* rmax = reinterpret_cast<double*>(koff + kt);
+  const int64_t rb = blockIdx.z, r0 = (int64_t)blockIdx.x * RB;
   int64_t b0, b1, b2;
   enumerate_batch(j, rb, b0, b1, b2);
   const cplx* base = j.ptr + j.bat(b0, b1, b2);
-  const int rl = threadIdx.x / 8, grp = threadIdx.x % 8;
-  if (threadIdx.x < TR) rmax[threadIdx.x] = 0.0;
-  for (int kt = 0; kt < nkt; ++kt) {
-    const int64_t kc = (int64_t)kt * TK;
-    tile_offsets(j, r0, kc, roff, koff);
-    __syncthreads();
-    load_slice_tile(j, base, roff, koff, r0, kc, tile);
-    __syncthreads();
-    double m = 0.0;
+  for (int i = threadIdx.x; i < RB + kt; i += SL_NT) {
+    if (i < RB) roff[i] = (r0 + i < j.R) ? j.rmap(r0 + i) : 0;
+    else koff[i - RB] = (i - RB < j.K) ? j.kmap(j.k0 + i - RB) : 0;
+  }
+  __syncthreads();
+  // stage the block's rows, eight loads in flight per thread
+  const int n = RB * kt;
+  for (int e0 = 0; e0 < n; e0 += 8 * SL_NT) {
+    cplx v[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const cplx v = tile[rl][tcol(grp * 8 + i)];
+      const int e = e0 + threadIdx.x + i * SL_NT;
+      int rl, kl;
+      if (j.r_fast) { rl = e % RB; kl = e / RB; } else { kl = e % kt; rl = e / kt; }
+      v[i] = cmk(0.0, 0.0);
+      if (e < n && r0 + rl < j.R && kl < j.K) v[i] = __ldg(base + roff[rl] + koff[kl]);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int e = e0 + threadIdx.x + i * SL_NT;
+      int rl, kl;
+      if (j.r_fast) { rl = e % RB; kl = e / RB; } else { kl = e % kt; rl = e / kt; }
+      if (j.conj) v[i].y = -v[i].y;
+      if (e < n) rows[rl * ld + tcol(kl)] = v[i];
+    }
+  }
+  __syncthreads();
+  // row maxima: SL_NT / RB consecutive threads per row
+  constexpr int TPR = SL_NT / RB;
+  static_assert(TPR <= 32 && (32 % TPR) == 0, "threads of a row within one warp");
+  {
+    const int rl = threadIdx.x / TPR, part = threadIdx.x % TPR;
+    double m = 0.0;
+    for (int k = part; k < kt; k += TPR) {
+      const cplx v = rows[rl * ld + tcol(k)];
       m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
     }
-    for (int o = 4; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (grp == 0) rmax[rl] = fmax(rmax[rl], m);
-    __syncthreads();
+    for (int o = TPR / 2; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (part == 0) rmax[rl] = m;
   }
-  const int64_t r = r0 + rl;
-  int e = 0;
-  if (rmax[rl] > 0.0) {
-    frexp(rmax[rl], &e);
-    ++e;  // one bit of headroom, as in slice_expo_kernel
-  }
-  if (grp == 0 && r < j.R) j.expo[rb * j.e_ld + r] = e;
-  for (int kt = 0; kt < nkt; ++kt) {
-    const int64_t kc = (int64_t)kt * TK;
-    tile_offsets(j, r0, kc, roff, koff);
-    __syncthreads();
-    load_slice_tile(j, base, roff, koff, r0, kc, tile);
-    __syncthreads();
+  __syncthreads();
+  // digits: one thread per (row, 8 consecutive K positions)
+  const int groups = kt / 8;
+  for (int it = threadIdx.x; it < RB * groups; it += SL_NT) {
+    const int rl = it / groups, g = it % groups;
+    const int64_t r = r0 + rl;
+    int e = 0;
+    if (rmax[rl] > 0.0) {
+      frexp(rmax[rl], &e);
+      ++e;  // one bit of headroom, as in slice_expo_kernel
+    }
+    if (g == 0 && r < j.R) j.expo[rb * j.e_ld + r] = e;
     cplx vals[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) vals[i] = tile[rl][tcol(grp * 8 + i)];
-    __syncthreads();  // the next tile overwrites `tile`
-    write_digits(j, vals, rb, r, kc + grp * 8, e);
+    for (int i = 0; i < 8; ++i) vals[i] = rows[rl * ld + tcol(g * 8 + i)];
+    write_digits(j, vals, rb, r, (int64_t)g * 8, e);
   }
 }
 
@@ -987,6 +1019,22 @@ int max_bn(int S, int cols) {
 
 unsigned blocks_for(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)); }
 
+// Opt-in shared memory above 48 KB for the kernels that use it (once per engine).
+void set_smem_attrs(SplitEngine& se) {
+  if (se.attr_set) return;
+  const void* fns[] = {
+      (const void*)split_gemm_tc_kernel<2, false>, (const void*)split_gemm_tc_kernel<3, false>,
+      (const void*)split_gemm_tc_kernel<4, false>, (const void*)split_gemm_tc_kernel<5, false>,
+      (const void*)split_gemm_tc_kernel<6, false>, (const void*)split_gemm_tc_kernel<7, false>,
+      (const void*)split_gemm_tc_kernel<8, false>, (const void*)split_gemm_tc_kernel<2, true>,
+      (const void*)split_gemm_tc_kernel<3, true>,  (const void*)split_gemm_tc_kernel<4, true>,
+      (const void*)split_gemm_tc_kernel<5, true>,  (const void*)split_gemm_tc_kernel<6, true>,
+      (const void*)split_gemm_tc_kernel<7, true>,  (const void*)split_gemm_tc_kernel<8, true>,
+      (const void*)slice_resident_kernel<8>,       (const void*)slice_resident_kernel<16>};
+  for (const void* f : fns) GB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+  se.attr_set = true;
+}
+
 // Slice one operand (rows x K) into planes + exponents.
 void run_slicer(SliceJob& j, int64_t nrb, cudaStream_t st) {
   const int64_t ne = nrb * j.e_ld;
@@ -1002,9 +1050,17 @@ void run_slicer(SliceJob& j, int64_t nrb, cudaStream_t st) {
   j.single = 0;
   const int64_t nkt = (j.kpad / 2 + TK - 1) / TK;  // K tiles covering the padded range
   if (nkt <= 8) {
-    // moderate contraction length: one block per TR rows does both passes
-    dim3 g((unsigned)((j.rpad + TR - 1) / TR), 1, (unsigned)nrb);
-    slice_fused_kernel<<<g, SL_NT, 0, st>>>(j, (int)nkt);
+    // moderate contraction length: the block's rows stay in shared memory for both steps
+    const int kt = (int)nkt * TK;
+    if (nkt <= 4) {
+      const size_t sm = resident_smem(16, kt);
+      dim3 g((unsigned)((j.rpad + 15) / 16), 1, (unsigned)nrb);
+      slice_resident_kernel<16><<<g, SL_NT, sm, st>>>(j, kt);
+    } else {
+      const size_t sm = resident_smem(8, kt);
+      dim3 g((unsigned)((j.rpad + 7) / 8), 1, (unsigned)nrb);
+      slice_resident_kernel<8><<<g, SL_NT, sm, st>>>(j, kt);
+    }
     GB_CHECK_LAUNCH();
     return;
   }
@@ -1055,6 +1111,7 @@ struct Prepared {
 // parameters (and, for the tensor-core engine, its tensor maps).
 Prepared prepare_chunk(SplitEngine& se, const ZGemm& g0, int S, int BN, int64_t k0, int64_t Kc, cudaStream_t st) {
   Prepared pr;
+  set_smem_attrs(se);
   int depA[3], depB[3];
   deps_of(g0.A, depA);
   deps_of(g0.B, depB);
@@ -1131,15 +1188,6 @@ Prepared prepare_chunk(SplitEngine& se, const ZGemm& g0, int S, int BN, int64_t 
 }
 
 template <bool G>
-void set_smem_attrs() {
-  const void* fns[] = {(const void*)split_gemm_tc_kernel<2, G>, (const void*)split_gemm_tc_kernel<3, G>,
-                       (const void*)split_gemm_tc_kernel<4, G>, (const void*)split_gemm_tc_kernel<5, G>,
-                       (const void*)split_gemm_tc_kernel<6, G>, (const void*)split_gemm_tc_kernel<7, G>,
-                       (const void*)split_gemm_tc_kernel<8, G>};
-  for (const void* f : fns) GB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
-}
-
-template <bool G>
 void launch_tc(int S, unsigned grid, size_t smem, cudaStream_t st, const CUtensorMap& mA, const CUtensorMap& mB,
                const GemmParams& p) {
   switch (S) {
@@ -1210,11 +1258,6 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st, i
     }
     size_t smem = 0;
     ring_layout(S, BN, pr.p, smem);
-    if (!se.attr_set) {
-      set_smem_attrs<false>();
-      set_smem_attrs<true>();
-      se.attr_set = true;
-    }
     KernelRecord* rec = begin_record(c, pr.flops, st);
     launch_tc<false>(S, persistent_grid(c, pr.ntiles), smem, st, pr.mA, pr.mB, pr.p);
     if (rec) GB_CUDA(cudaEventRecord(rec->stop, st));
@@ -1245,11 +1288,6 @@ void split_gemm_group(const std::vector<Context*>& cs, const std::vector<ZGemm>&
     return;
   }
   SplitEngine& se0 = *ses[0];
-  if (!se0.attr_set) {
-    set_smem_attrs<false>();
-    set_smem_attrs<true>();
-    se0.attr_set = true;
-  }
   // K chunk ch of every problem that has one, all in one grouped launch per chunk
   for (int64_t ch = 0; ch < nch; ++ch) {
     std::vector<GroupEntry> entries;

@@ -113,6 +113,19 @@ struct ZResult {
   BatchMap bat;
 };
 
+// Split precision: per-row exponents of a later contraction's operand, recorded by the
+// contraction that produces that operand.  A result element in column n of batch (b0, b1, b2)
+// belongs to entry  c0 b0 + c1 b1 + c2 b2 + ((n / d1) % m1) s1 + (n / d2) s2  of `expo`; every
+// result row folds into the same entry.  Aligned groups of 8 columns must share an entry (d1 and
+// d2 multiples of 8 where their term is used).
+struct ExpoSink {
+  int32_t* expo = nullptr;  // nullptr: no sink
+  int64_t c0 = 0, c1 = 0, c2 = 0;
+  int64_t d1 = 1, m1 = 1, s1 = 0;
+  int64_t d2 = 1, s2 = 0;
+  int64_t count = 0;  // entries of `expo`
+};
+
 // C = alpha * op(A) op(B) + beta * C over a 3-level batch.
 struct ZGemm {
   int64_t M = 0, N = 0, K = 0;
@@ -121,6 +134,12 @@ struct ZGemm {
   ZResult C;      // M x N
   cplx alpha = {1.0, 0.0};
   cplx beta = {0.0, 0.0};
+  // split precision only: `sink` records the exponents of a later contraction's operand from this
+  // result (a single K chunk, beta = 0, alpha a real power of two); `B_expo` holds operand B's
+  // column exponents, written by such a sink, B_expo_ld apart per reduced batch of B
+  ExpoSink sink;
+  int32_t* B_expo = nullptr;
+  int64_t B_expo_ld = 0;
 };
 
 void zgemm_fp64(const ZGemm& g, cudaStream_t st);

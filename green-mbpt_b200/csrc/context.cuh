@@ -57,7 +57,7 @@ enum ScratchSlot {
   SL_IO_S1, SL_IO_H, SL_DM, SL_PINV, SL_SPLIT0, SL_HF_TAB, SL_X2C_DM, SL_X2C_S, SL_X2C_F, SL_X2C_GAB, SL_X2C_GBA,
   SL_X2C_SIG, SL_Q0_Y, SL_Q0_T, SL_Q0_D, SL_Q0_E, SL_Q0_S, SL_ADJ_TH, SL_ADJ_PTW, SL_ADJ_W, SL_ADJ_WB,
   SL_ADJ_PTWB, SL_ADJ_PWB, SL_ADJ_THB, SL_ADJ_XB, SL_ADJ_AB, SL_ADJ_P0B, SL_ADJ_P0HB, SL_ADJ_X3, SL_ADJ_TAB, SL_ADJ_TQ, SL_ADJ_VBF, SL_ADJ_VBH,
-  SL_COUNT
+  SL_SINK, SL_COUNT
 };
 
 struct SplitEngine;

@@ -309,6 +309,13 @@ struct GwRun {
   int64_t per_k_sigma = 0;
   cplx *P0 = nullptr, *Pw = nullptr, *Pinv = nullptr, *aug = nullptr, *X1 = nullptr, *X2 = nullptr;
   int q0 = 0, q1 = 0;
+  // exponent sink (split precision on the tensor cores): (e) records the column exponents of Y2
+  // for (f) as it stores Y2, so that slicing Y2 needs no separate exponent pass.  Measured on the
+  // c2 shapes it costs (e) about 0.4 of the pass it saves; in the epilogue-bound (b) it would cost
+  // more than the pass for Bt, so (b) -> (c) keeps the pass.
+  bool sink_s = false;
+  int32_t* sink = nullptr;
+  int64_t sink_ld_s = 0;
 
   GwRun(Context& c_, const cplx* G_, cplx* Sigma_, cudaStream_t st_) : c(c_), st(st_), d(c_.d) {
     require(d.nts % 2 == 0, GB200_ERR_WRONG_GRID, "Number of tau points should be even!!!");
@@ -347,6 +354,12 @@ struct GwRun {
     aug = (cplx*)c.scratch.get(SL_AUG, (size_t)nw_b * NQ * 2 * NQ * sizeof(cplx));
     X1 = (cplx*)c.scratch.get(SL_Y1, (size_t)kb * per_k_sigma * sizeof(cplx));
     X2 = (cplx*)c.scratch.get(SL_Y2, (size_t)kb * per_k_sigma * sizeof(cplx));
+    if (c.prec_mode == GB200_PREC_SPLIT && c.split_core == 0 && nao % 8 == 0) {
+      auto slices_of = [&](int stage) { return c.contraction_slices[stage] > 0 ? c.contraction_slices[stage] : c.slices; };
+      sink_s = NQ <= split_max_chunk(slices_of(4));
+      sink_ld_s = (int64_t)nts * ns * nao;
+      if (sink_s) sink = (int32_t*)c.scratch.get(SL_SINK, (size_t)kb * sink_ld_s * sizeof(int32_t));
+    }
     if (c.q0_on) {
       require(c.q_begin <= 0 && (c.q_end < 0 || c.q_end >= nk), GB200_ERR_INVALID,
               "q0 correction: needs all q-points in one context (it extrapolates over q)");
@@ -494,6 +507,14 @@ struct GwRun {
     f.C.ptr = Sigma + (int64_t)k0 * ge; f.C.row = lin(1); f.C.col = two(nao, nao, g_s);
     f.C.bat.s0 = ge;
     f.alpha = cmk(-1.0, 0.0); f.beta = cmk(1.0, 0.0);
+    if (sink_s) {
+      // column ((t,s),i) of (f)'s B in batch kk: Y2[kk][t][s][i][*], i.e. (e)'s columns
+      // (kk,(i,n)) in its batch (t, s): entry kk ld + (t ns + s) nao + i
+      e.sink.expo = sink; e.sink.c1 = (int64_t)ns * nao; e.sink.c2 = nao;
+      e.sink.d1 = nao; e.sink.m1 = nao; e.sink.s1 = 1; e.sink.d2 = nao2; e.sink.s2 = sink_ld_s;
+      e.sink.count = (int64_t)kbk * sink_ld_s;
+      f.B_expo = sink; f.B_expo_ld = sink_ld_s;
+    }
     out[0] = dd;
     out[1] = e;
     out[2] = f;

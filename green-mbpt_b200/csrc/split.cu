@@ -30,6 +30,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -190,6 +191,7 @@ struct GemmParams {
   cplx alpha, beta;
   int alpha_pow2;  // alpha is real and a power of two (possibly negative)
   int pair;        // the chunk is short enough that diagonal pairs (0,1), (2,3) fit int32 exactly
+  ExpoSink sink;   // exponents of a later contraction's operand, folded from the stored results
   int* err;
   // grouped launch: the problems' entries (tile ranges in order) and the total tile count; the
   // launch-wide fields above (S, BN = the widest tile, stages, nbuf, err) size the shared ring
@@ -605,7 +607,8 @@ __host__ __device__ inline SmemLayout smem_layout(int S, int BN, int stages) {
   return L;
 }
 
-// one set of per-tile epilogue tables: row and column offsets of C, column factors, exponents
+// one set of per-tile epilogue tables: row and column offsets of C, column factors, row exponents
+// and the exponent-sink entries of the column groups (BN / 8 of the BN 4-byte slots at the end)
 __host__ __device__ inline int table_set_bytes(int BN) {
   return ((TILE_M / 2) * 8 + BN * 16 + (TILE_M / 2 + BN) * 4 + 15) / 16 * 16;
 }
@@ -644,7 +647,7 @@ __device__ __forceinline__ TileCoord tile_coord(const GemmParams& p, int64_t t) 
 //  warp 1       MMA issuer (one thread), `nbuf` TMEM accumulator sets of S * BN columns
 //  warps 2..    epilogue (EPI_WARPS): TMEM -> registers -> FP64 recombination -> stores to C
 // With nbuf = 2 the epilogue of one tile overlaps the MMAs of the next.
-template <int SS, bool GROUPED>
+template <int SS, bool GROUPED, bool SINK>
 __global__ void __launch_bounds__(NWARPS * 32, 1)
     split_gemm_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, GemmParams p) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -805,9 +808,16 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
       int64_t* sh_colC = sh_rowC + TILE_M / 2;
       double* sh_csc = reinterpret_cast<double*>(sh_colC + q.BN);  // column factors 2^(eb - 7(S+1))
       int32_t* sh_eA = reinterpret_cast<int32_t*>(sh_csc + q.BN);
+      int32_t* sh_key = sh_eA + TILE_M / 2;  // exponent-sink entry per group of 8 columns
       // (filled while the MMAs of this tile run)
-      for (int i = et; i < TILE_M / 2 + q.BN; i += EPI_THREADS) {
-        if (i < TILE_M / 2) {
+      const int ntab = TILE_M / 2 + q.BN + ((SINK && q.sink.expo) ? q.BN / EPI_CG : 0);
+      for (int i = et; i < ntab; i += EPI_THREADS) {
+        if (i >= TILE_M / 2 + q.BN) {
+          const int64_t n = tc.ncol0 + (int64_t)(i - TILE_M / 2 - q.BN) * EPI_CG;
+          const ExpoSink& sk = q.sink;
+          sh_key[i - TILE_M / 2 - q.BN] = (int32_t)(sk.c0 * tc.b0 + sk.c1 * tc.b1 + sk.c2 * tc.b2 +
+                                                    ((n / sk.d1) % sk.m1) * sk.s1 + (n / sk.d2) * sk.s2);
+        } else if (i < TILE_M / 2) {
           const int64_t m = tc.mrow0 / 2 + i;
           sh_eA[i] = m < q.M ? q.eA[tc.rbA * q.eA_ld + m] : 0;
           sh_rowC[i] = m < q.M ? q.C.row(m) : 0;
@@ -879,6 +889,28 @@ __global__ void __launch_bounds__(NWARPS * 32, 1)
                 if (has_beta) val = cadd(val, cmul(q.beta, *d));
                 *d = val;
               }
+            }
+          }
+          if constexpr (SINK) {
+            if (q.sink.expo) {
+              // exponent of the largest stored |Re|, |Im| of the warp's 8 columns (one aligned group,
+              // one entry), with the convention of slice_expo_kernel; the host allows sinks only
+              // where the stored value is v itself (alpha a power of two folded into rs, beta = 0)
+              double smax = 0.0;
+              if (mok) {
+#pragma unroll
+                for (int j = 0; j < EPI_CG; ++j)
+                  if (c0 + cc + j < nlim) smax = fmax(smax, fabs(v[j]));
+              }
+              int ev = INT_MIN;
+              if (smax > 0.0) {
+                const int biased = (int)((__double_as_longlong(smax) >> 52) & 0x7FF);
+                int ex = biased - 1022;  // frexp's exponent for a normal number
+                if (biased == 0) frexp(smax, &ex);
+                ev = ex + 1;
+              }
+              ev = __reduce_max_sync(0xffffffffu, ev);
+              if (lane == 0 && ev != INT_MIN) atomicMax(q.sink.expo + sh_key[(c0 + cc) / EPI_CG], ev);
             }
           }
         }
@@ -1023,14 +1055,14 @@ unsigned blocks_for(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<
 void set_smem_attrs(SplitEngine& se) {
   if (se.attr_set) return;
   const void* fns[] = {
-      (const void*)split_gemm_tc_kernel<2, false>, (const void*)split_gemm_tc_kernel<3, false>,
-      (const void*)split_gemm_tc_kernel<4, false>, (const void*)split_gemm_tc_kernel<5, false>,
-      (const void*)split_gemm_tc_kernel<6, false>, (const void*)split_gemm_tc_kernel<7, false>,
-      (const void*)split_gemm_tc_kernel<8, false>, (const void*)split_gemm_tc_kernel<2, true>,
-      (const void*)split_gemm_tc_kernel<3, true>,  (const void*)split_gemm_tc_kernel<4, true>,
-      (const void*)split_gemm_tc_kernel<5, true>,  (const void*)split_gemm_tc_kernel<6, true>,
-      (const void*)split_gemm_tc_kernel<7, true>,  (const void*)split_gemm_tc_kernel<8, true>,
-      (const void*)slice_resident_kernel<8>,       (const void*)slice_resident_kernel<16>};
+#define GB_TC_ALL(G, K)                                                                    \
+  (const void*)split_gemm_tc_kernel<2, G, K>, (const void*)split_gemm_tc_kernel<3, G, K>, \
+      (const void*)split_gemm_tc_kernel<4, G, K>, (const void*)split_gemm_tc_kernel<5, G, K>, \
+      (const void*)split_gemm_tc_kernel<6, G, K>, (const void*)split_gemm_tc_kernel<7, G, K>, \
+      (const void*)split_gemm_tc_kernel<8, G, K>
+      GB_TC_ALL(false, false), GB_TC_ALL(false, true), GB_TC_ALL(true, false), GB_TC_ALL(true, true),
+#undef GB_TC_ALL
+      (const void*)slice_resident_kernel<8>, (const void*)slice_resident_kernel<16>};
   for (const void* f : fns) GB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
   se.attr_set = true;
 }
@@ -1075,6 +1107,18 @@ void run_slicer(SliceJob& j, int64_t nrb, cudaStream_t st) {
   slice_write_kernel<<<g2, SL_NT, 0, st>>>(j);
   GB_CHECK_LAUNCH();
   fix_empty_expo_kernel<<<blocks_for(ne), 256, 0, st>>>(j.expo, ne);
+  GB_CHECK_LAUNCH();
+}
+
+// The digit pass alone, with the exponents already in j.expo (empty rows marked EXP_EMPTY).
+void run_slicer_known_expo(SliceJob& j, int64_t nrb, cudaStream_t st) {
+  require(nrb < 65536, GB200_ERR_INVALID, "split: too many operand batches");
+  j.single = 0;
+  dim3 g((unsigned)((j.rpad + TR - 1) / TR), (unsigned)((j.kpad / 2 + TK - 1) / TK), (unsigned)nrb);
+  require(g.y < 65536, GB200_ERR_INVALID, "split: contraction too long for the slicer grid");
+  slice_write_kernel<<<g, SL_NT, 0, st>>>(j);
+  GB_CHECK_LAUNCH();
+  fix_empty_expo_kernel<<<blocks_for(nrb * j.e_ld), 256, 0, st>>>(j.expo, nrb * j.e_ld);
   GB_CHECK_LAUNCH();
 }
 
@@ -1146,7 +1190,29 @@ Prepared prepare_chunk(SplitEngine& se, const ZGemm& g0, int S, int BN, int64_t 
     j.embed = 0; j.S = S; j.rows_pad = rowsB_pad; j.rpad = rowsB_pad; j.kpad = kpad; j.e_ld = rowsB_pad;
     j.out = se.planesB.p; j.expo = se.expB.p;
     j.r_fast = std::abs(g0.B.col.s_in) < std::abs(g0.B.row.s_in);
-    run_slicer(j, nrbB, st);
+    if (g0.B_expo) {
+      // the producer of B recorded its column exponents (over the whole K range, so every chunk
+      // can use them): only the digit pass runs
+      require(g0.B_expo_ld >= g0.N, GB200_ERR_INVALID, "split: exponent array of B too short");
+      j.expo = g0.B_expo;
+      j.e_ld = g0.B_expo_ld;
+      run_slicer_known_expo(j, nrbB, st);
+    } else {
+      run_slicer(j, nrbB, st);
+    }
+  }
+  if (g0.sink.expo) {
+    int aexp = 0;
+    require(se.core == 0, GB200_ERR_INVALID, "split: exponent sinks need the tensor-core engine");
+    require(k0 == 0 && Kc == g0.K, GB200_ERR_INVALID, "split: an exponent sink needs a single K chunk");
+    require(g0.beta.x == 0.0 && g0.beta.y == 0.0 && g0.alpha.y == 0.0 && g0.alpha.x != 0.0 &&
+                std::fabs(std::frexp(g0.alpha.x, &aexp)) == 0.5,
+            GB200_ERR_INVALID, "split: an exponent sink needs beta = 0 and a real power-of-two alpha");
+    require((g0.sink.s1 == 0 || g0.sink.d1 % 8 == 0) && (g0.sink.s2 == 0 || g0.sink.d2 % 8 == 0), GB200_ERR_INVALID,
+            "split: sink entries must be constant over aligned groups of 8 columns");
+    require(g0.sink.count < (1LL << 31), GB200_ERR_INVALID, "split: exponent sink too large");
+    fill_int_kernel<<<blocks_for(g0.sink.count), 256, 0, st>>>(g0.sink.expo, g0.sink.count, EXP_EMPTY);
+    GB_CHECK_LAUNCH();
   }
   GemmParams& p = pr.p;
   p.S = S; p.BN = BN; p.nkb = (int)(kpad / KBLK);
@@ -1155,6 +1221,11 @@ Prepared prepare_chunk(SplitEngine& se, const ZGemm& g0, int S, int BN, int64_t 
   std::copy(depB, depB + 3, p.depB);
   p.rowsA_pad = rowsA_pad; p.rowsB_pad = rowsB_pad;
   p.eA = se.expA.p; p.eB = se.expB.p; p.eA_ld = rowsA_pad / 2; p.eB_ld = rowsB_pad;
+  if (g0.B_expo) {
+    p.eB = g0.B_expo;
+    p.eB_ld = g0.B_expo_ld;
+  }
+  p.sink = g0.sink;
   p.C = g0.C; p.alpha = g0.alpha; p.beta = (k0 == 0) ? g0.beta : cmk(1.0, 0.0);
   p.err = se.err.p;
   {
@@ -1187,19 +1258,27 @@ Prepared prepare_chunk(SplitEngine& se, const ZGemm& g0, int S, int BN, int64_t 
   return pr;
 }
 
-template <bool G>
-void launch_tc(int S, unsigned grid, size_t smem, cudaStream_t st, const CUtensorMap& mA, const CUtensorMap& mB,
-               const GemmParams& p) {
+template <bool G, bool K>
+void launch_tc_s(int S, unsigned grid, size_t smem, cudaStream_t st, const CUtensorMap& mA, const CUtensorMap& mB,
+                 const GemmParams& p) {
   switch (S) {
-    case 2: split_gemm_tc_kernel<2, G><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
-    case 3: split_gemm_tc_kernel<3, G><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
-    case 4: split_gemm_tc_kernel<4, G><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
-    case 5: split_gemm_tc_kernel<5, G><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
-    case 6: split_gemm_tc_kernel<6, G><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
-    case 7: split_gemm_tc_kernel<7, G><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
-    default: split_gemm_tc_kernel<8, G><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+    case 2: split_gemm_tc_kernel<2, G, K><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+    case 3: split_gemm_tc_kernel<3, G, K><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+    case 4: split_gemm_tc_kernel<4, G, K><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+    case 5: split_gemm_tc_kernel<5, G, K><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+    case 6: split_gemm_tc_kernel<6, G, K><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+    case 7: split_gemm_tc_kernel<7, G, K><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
+    default: split_gemm_tc_kernel<8, G, K><<<grid, NWARPS * 32, smem, st>>>(mA, mB, p); break;
   }
   GB_CHECK_LAUNCH();
+}
+
+// `sink`: some problem of the launch records exponents (otherwise the kernel without that code)
+template <bool G>
+void launch_tc(int S, bool sink, unsigned grid, size_t smem, cudaStream_t st, const CUtensorMap& mA,
+               const CUtensorMap& mB, const GemmParams& p) {
+  if (sink) launch_tc_s<G, true>(S, grid, smem, st, mA, mB, p);
+  else launch_tc_s<G, false>(S, grid, smem, st, mA, mB, p);
 }
 
 // Launch-wide layout for tiles up to BN columns: TMA ring depth (what fits, at most 6 K blocks)
@@ -1259,10 +1338,12 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g0, cudaStream_t st, i
     size_t smem = 0;
     ring_layout(S, BN, pr.p, smem);
     KernelRecord* rec = begin_record(c, pr.flops, st);
-    launch_tc<false>(S, persistent_grid(c, pr.ntiles), smem, st, pr.mA, pr.mB, pr.p);
+    launch_tc<false>(S, pr.p.sink.expo != nullptr, persistent_grid(c, pr.ntiles), smem, st, pr.mA, pr.mB, pr.p);
     if (rec) GB_CUDA(cudaEventRecord(rec->stop, st));
   }
 }
+
+int64_t split_max_chunk(int slices) { return kmax_for(slices); }
 
 void split_gemm_group(const std::vector<Context*>& cs, const std::vector<ZGemm>& gs, cudaStream_t st, int slices) {
   require(cs.size() == gs.size() && !cs.empty(), GB200_ERR_INVALID, "split group: one contraction per context");
@@ -1294,6 +1375,7 @@ void split_gemm_group(const std::vector<Context*>& cs, const std::vector<ZGemm>&
     int BNmax = 16;
     double flops = 0.0;
     int64_t total = 0;
+    bool sink = false;
     for (size_t i = 0; i < cs.size(); ++i) {
       const int64_t k0 = ch * kmax;
       if (k0 >= gs[i].K) continue;
@@ -1307,6 +1389,7 @@ void split_gemm_group(const std::vector<Context*>& cs, const std::vector<ZGemm>&
       total += pr.ntiles;
       BNmax = std::max(BNmax, bns[i]);
       flops += pr.flops;
+      sink = sink || pr.p.sink.expo != nullptr;
     }
     GemmParams p{};
     p.S = S;
@@ -1320,7 +1403,7 @@ void split_gemm_group(const std::vector<Context*>& cs, const std::vector<ZGemm>&
     p.ngroup = (int)entries.size();
     p.ntiles = total;
     KernelRecord* rec = begin_record(*cs[0], flops, st);
-    launch_tc<true>(S, persistent_grid(*cs[0], total), smem, st, entries[0].mA, entries[0].mB, p);
+    launch_tc<true>(S, sink, persistent_grid(*cs[0], total), smem, st, entries[0].mA, entries[0].mB, p);
     if (rec) GB_CUDA(cudaEventRecord(rec->stop, st));
   }
 }

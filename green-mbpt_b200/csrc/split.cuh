@@ -20,6 +20,9 @@ void split_gemm(Context& c, SplitEngine& se, const ZGemm& g, cudaStream_t st, in
 // persistent tensor-core launch per K chunk walks the tiles of all of them.
 void split_gemm_group(const std::vector<Context*>& cs, const std::vector<ZGemm>& gs, cudaStream_t st, int slices);
 void split_release(Context& c);
+// Longest K range one split launch takes without chunking (a contraction with an exponent sink
+// must fit it).
+int64_t split_max_chunk(int slices);
 // Non-zero if a split kernel hit a bounded-wait timeout since the last check (flag is cleared).
 int split_check_error(Context& c, cudaStream_t st);
 

@@ -346,56 +346,51 @@ __global__ void __launch_bounds__(SL_NT, 4) slice_expo_kernel(SliceJob j) {
 // of headroom in the row exponent e (split_digits.cuh).
 
 // Write the S digit planes of 8 consecutive K positions (from k) of row r with row exponent e,
-// including the zero padding of rows and K.
+// including the zero padding of rows and K.  S is a compile-time constant, so every digit shift is
+// a constant and one plane's 16 bytes take four packed words (balanced_digit_word).
+template <int S>
 __device__ __forceinline__ void write_digits(const SliceJob& j, const cplx (&vals)[8], int64_t rb, int64_t r, int64_t k,
                                              int e) {
   if (r >= j.rpad || 2 * k >= j.kpad) return;
-  const int S = j.S;
   // 2^(7S - e) in two exact power-of-two factors (the exponent can exceed the double range
   // for rows of tiny magnitude)
   const int ex = 7 * S - e;
   const int ex1 = max(-1000, min(1000, ex));
   const double sc1 = __longlong_as_double((long long)(ex1 + 1023) << 52);
   const double sc2 = __longlong_as_double((long long)(max(-1022, min(1023, ex - ex1)) + 1023) << 52);
-  // X + bias of the rounded scaled values (two's complement wrap-around gives X + bias >= 0)
-  const uint64_t bias = balanced_bias(S);
-  uint64_t ur[8], ui[8];
+  // X + bias of the rounded scaled values, (re, im) of the 8 positions in turn
+  uint64_t u[16];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
-    const cplx v = vals[i];
-    ur[i] = (uint64_t)__double2ll_rn((v.x * sc1) * sc2) + bias;
-    ui[i] = (uint64_t)__double2ll_rn((v.y * sc1) * sc2) + bias;
+    u[2 * i] = balanced_input((vals[i].x * sc1) * sc2, S);
+    u[2 * i + 1] = balanced_input((vals[i].y * sc1) * sc2, S);
   }
   const int64_t plane = j.rows_pad * j.kpad;
   int8_t* outb = j.out + rb * (int64_t)S * plane;
-  for (int s = 0; s < S; ++s) {
-    uint32_t w0[4], w1[4];
 #pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const uint32_t r0b = balanced_digit_byte(ur[2 * h], S, s);
-      const uint32_t i0b = balanced_digit_byte(ui[2 * h], S, s);
-      const uint32_t r1b = balanced_digit_byte(ur[2 * h + 1], S, s);
-      const uint32_t i1b = balanced_digit_byte(ui[2 * h + 1], S, s);
-      if (j.embed) {
-        // row 2r: (re, -im) pairs; row 2r+1: (im, re) pairs
-        const uint32_t ni0 = (0u - i0b) & 0xFFu, ni1 = (0u - i1b) & 0xFFu;
-        w0[h] = r0b | (ni0 << 8) | (r1b << 16) | (ni1 << 24);
-        w1[h] = i0b | (r0b << 8) | (i1b << 16) | (r1b << 24);
-      } else {
-        w0[h] = r0b | (i0b << 8) | (r1b << 16) | (i1b << 24);
-      }
-    }
+  for (int s = 0; s < S; ++s) {
+    uint32_t w[4];  // bytes (re, im) of positions 2h and 2h + 1
+#pragma unroll
+    for (int h = 0; h < 4; ++h) w[h] = balanced_digit_word(u[4 * h], u[4 * h + 1], u[4 * h + 2], u[4 * h + 3], S, s);
     int8_t* p = outb + (int64_t)s * plane;
     if (j.embed) {
+      // row 2r: (re, -im) pairs; row 2r+1: (im, re) pairs
+      uint32_t w0[4], w1[4];
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        w0[h] = __byte_perm(w[h], negate_bytes(w[h]), 0x7250);
+        w1[h] = __byte_perm(w[h], 0u, 0x2301);
+      }
       *reinterpret_cast<uint4*>(p + (2 * r) * j.kpad + 2 * k) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
       *reinterpret_cast<uint4*>(p + (2 * r + 1) * j.kpad + 2 * k) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
     } else {
-      *reinterpret_cast<uint4*>(p + r * j.kpad + 2 * k) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
+      *reinterpret_cast<uint4*>(p + r * j.kpad + 2 * k) = make_uint4(w[0], w[1], w[2], w[3]);
     }
   }
 }
 
 // Pass 2: slice planes, including the zero padding of rows and K.
+template <int S>
 __global__ void __launch_bounds__(SL_NT, 4) slice_write_kernel(SliceJob j) {
   __shared__ cplx tile[TR][TKP];
   __shared__ int64_t roff[TR], koff[TK];
@@ -429,7 +424,7 @@ __global__ void __launch_bounds__(SL_NT, 4) slice_write_kernel(SliceJob j) {
     e = j.expo[rb * j.e_ld + r];
     if (e == EXP_EMPTY) e = 0;
   }
-  write_digits(j, vals, rb, r, k, e);
+  write_digits<S>(j, vals, rb, r, k, e);
 }
 
 // One pass for contractions of moderate length (K up to 8 tiles): a block stages RB rows over the
@@ -443,7 +438,7 @@ inline size_t resident_smem(int rb, int kt) {
   return (size_t)rb * resident_ld(kt) * sizeof(cplx) + (size_t)(rb + kt) * sizeof(int64_t) + rb * sizeof(double);
 }
 
-template <int RB>
+template <int RB, int S>
 __global__ void __launch_bounds__(SL_NT) slice_resident_kernel(SliceJob j, int kt) {
   extern __shared__ __align__(16) uint8_t sl_smem[];
   const int ld = resident_ld(kt);
@@ -510,7 +505,7 @@ __global__ void __launch_bounds__(SL_NT) slice_resident_kernel(SliceJob j, int k
     cplx vals[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) vals[i] = rows[rl * ld + tcol(g * 8 + i)];
-    write_digits(j, vals, rb, r, (int64_t)g * 8, e);
+    write_digits<S>(j, vals, rb, r, (int64_t)g * 8, e);
   }
 }
 
@@ -1051,6 +1046,33 @@ int max_bn(int S, int cols) {
 
 unsigned blocks_for(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8)); }
 
+// the digit-writing kernels for the job's slice count (a template parameter of the kernels)
+void launch_write(const SliceJob& j, dim3 g, cudaStream_t st) {
+  switch (j.S) {
+    case 2: slice_write_kernel<2><<<g, SL_NT, 0, st>>>(j); break;
+    case 3: slice_write_kernel<3><<<g, SL_NT, 0, st>>>(j); break;
+    case 4: slice_write_kernel<4><<<g, SL_NT, 0, st>>>(j); break;
+    case 5: slice_write_kernel<5><<<g, SL_NT, 0, st>>>(j); break;
+    case 6: slice_write_kernel<6><<<g, SL_NT, 0, st>>>(j); break;
+    case 7: slice_write_kernel<7><<<g, SL_NT, 0, st>>>(j); break;
+    default: slice_write_kernel<8><<<g, SL_NT, 0, st>>>(j); break;
+  }
+  GB_CHECK_LAUNCH();
+}
+
+template <int RB>
+void launch_resident(const SliceJob& j, dim3 g, size_t sm, int kt, cudaStream_t st) {
+  switch (j.S) {
+    case 2: slice_resident_kernel<RB, 2><<<g, SL_NT, sm, st>>>(j, kt); break;
+    case 3: slice_resident_kernel<RB, 3><<<g, SL_NT, sm, st>>>(j, kt); break;
+    case 4: slice_resident_kernel<RB, 4><<<g, SL_NT, sm, st>>>(j, kt); break;
+    case 5: slice_resident_kernel<RB, 5><<<g, SL_NT, sm, st>>>(j, kt); break;
+    case 6: slice_resident_kernel<RB, 6><<<g, SL_NT, sm, st>>>(j, kt); break;
+    case 7: slice_resident_kernel<RB, 7><<<g, SL_NT, sm, st>>>(j, kt); break;
+    default: slice_resident_kernel<RB, 8><<<g, SL_NT, sm, st>>>(j, kt); break;
+  }
+}
+
 // Opt-in shared memory above 48 KB for the kernels that use it (once per engine).
 void set_smem_attrs(SplitEngine& se) {
   if (se.attr_set) return;
@@ -1062,7 +1084,14 @@ void set_smem_attrs(SplitEngine& se) {
       (const void*)split_gemm_tc_kernel<8, G, K>
       GB_TC_ALL(false, false), GB_TC_ALL(false, true), GB_TC_ALL(true, false), GB_TC_ALL(true, true),
 #undef GB_TC_ALL
-      (const void*)slice_resident_kernel<8>, (const void*)slice_resident_kernel<16>};
+#define GB_RES_ALL(RB)                                                                        \
+  (const void*)slice_resident_kernel<RB, 2>, (const void*)slice_resident_kernel<RB, 3>,       \
+      (const void*)slice_resident_kernel<RB, 4>, (const void*)slice_resident_kernel<RB, 5>,   \
+      (const void*)slice_resident_kernel<RB, 6>, (const void*)slice_resident_kernel<RB, 7>,   \
+      (const void*)slice_resident_kernel<RB, 8>
+      GB_RES_ALL(8), GB_RES_ALL(16)
+#undef GB_RES_ALL
+  };
   for (const void* f : fns) GB_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
   se.attr_set = true;
 }
@@ -1075,8 +1104,7 @@ void run_slicer(SliceJob& j, int64_t nrb, cudaStream_t st) {
     // the whole contraction range fits one tile: one pass finds the exponents and writes the slices
     j.single = 1;
     dim3 g((unsigned)((j.rpad + TR - 1) / TR), 1, (unsigned)nrb);
-    slice_write_kernel<<<g, SL_NT, 0, st>>>(j);
-    GB_CHECK_LAUNCH();
+    launch_write(j, g, st);
     return;
   }
   j.single = 0;
@@ -1087,11 +1115,11 @@ void run_slicer(SliceJob& j, int64_t nrb, cudaStream_t st) {
     if (nkt <= 4) {
       const size_t sm = resident_smem(16, kt);
       dim3 g((unsigned)((j.rpad + 15) / 16), 1, (unsigned)nrb);
-      slice_resident_kernel<16><<<g, SL_NT, sm, st>>>(j, kt);
+      launch_resident<16>(j, g, sm, kt, st);
     } else {
       const size_t sm = resident_smem(8, kt);
       dim3 g((unsigned)((j.rpad + 7) / 8), 1, (unsigned)nrb);
-      slice_resident_kernel<8><<<g, SL_NT, sm, st>>>(j, kt);
+      launch_resident<8>(j, g, sm, kt, st);
     }
     GB_CHECK_LAUNCH();
     return;
@@ -1104,7 +1132,7 @@ void run_slicer(SliceJob& j, int64_t nrb, cudaStream_t st) {
   slice_expo_kernel<<<g1, SL_NT, 0, st>>>(j);
   GB_CHECK_LAUNCH();
   dim3 g2((unsigned)((j.rpad + TR - 1) / TR), (unsigned)((j.kpad / 2 + TK - 1) / TK), (unsigned)nrb);
-  slice_write_kernel<<<g2, SL_NT, 0, st>>>(j);
+  launch_write(j, g2, st);
   GB_CHECK_LAUNCH();
   fix_empty_expo_kernel<<<blocks_for(ne), 256, 0, st>>>(j.expo, ne);
   GB_CHECK_LAUNCH();
@@ -1116,7 +1144,7 @@ void run_slicer_known_expo(SliceJob& j, int64_t nrb, cudaStream_t st) {
   j.single = 0;
   dim3 g((unsigned)((j.rpad + TR - 1) / TR), (unsigned)((j.kpad / 2 + TK - 1) / TK), (unsigned)nrb);
   require(g.y < 65536, GB200_ERR_INVALID, "split: contraction too long for the slicer grid");
-  slice_write_kernel<<<g, SL_NT, 0, st>>>(j);
+  launch_write(j, g, st);
   GB_CHECK_LAUNCH();
   fix_empty_expo_kernel<<<blocks_for(nrb * j.e_ld), 256, 0, st>>>(j.expo, nrb * j.e_ld);
   GB_CHECK_LAUNCH();

@@ -116,7 +116,6 @@ struct Context {
 
   // per-q offset tables (device): [nq][nk] or [nq][nk*ns]
   DevArray<int64_t> tab_pair_plus, tab_pair_minus, tab_g_plus, tab_g_minus, tab_pair_plus_ns;
-  DevArray<int64_t> tab_pair_back_ns;  // V(k+q, k) per (q, k, spin): the pair of (c)'s operand
   DevArray<int64_t> tab_v_diag;  // pair subset: offset of block (k, k) in V per k (0 where not held)
 
   Scratch scratch;

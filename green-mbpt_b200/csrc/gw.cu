@@ -129,8 +129,7 @@ void build_tables(Context& c) {
   const int nk = c.d.nk, ns = c.ns_eff();
   const int64_t pe = c.pair_elems();
   const int64_t ge = (int64_t)c.d.nao * c.d.nao;
-  std::vector<int64_t> pp(nk * nk), pm(nk * nk), gp(nk * nk), gm(nk * nk), ppns((size_t)nk * nk * ns),
-      pbns((size_t)nk * nk * ns);
+  std::vector<int64_t> pp(nk * nk), pm(nk * nk), gp(nk * nk), gm(nk * nk), ppns((size_t)nk * nk * ns);
   for (int q = 0; q < nk; ++q)
     for (int k = 0; k < nk; ++k) {
       int kp = c.kplus[(size_t)k * nk + q];
@@ -141,19 +140,13 @@ void build_tables(Context& c) {
       pm[(size_t)q * nk + k] = std::max<int64_t>(0, c.v_block(k, km)) * pe;
       gp[(size_t)q * nk + k] = (int64_t)kp * ge;              // G(., ., k+q)
       gm[(size_t)q * nk + k] = (int64_t)km * ge;              // G(., ., k-q)
-      // V(k+q, k) = V(k+q, (k+q)-q): held wherever V(k', k'-q) is for every k'
-      const int64_t pb = std::max<int64_t>(0, c.v_block(kp, k)) * pe;
-      for (int s = 0; s < ns; ++s) {
-        ppns[((size_t)q * nk + k) * ns + s] = pp[(size_t)q * nk + k];
-        pbns[((size_t)q * nk + k) * ns + s] = pb;
-      }
+      for (int s = 0; s < ns; ++s) ppns[((size_t)q * nk + k) * ns + s] = pp[(size_t)q * nk + k];
     }
   c.tab_pair_plus.upload(pp.data(), pp.size(), c.stream);
   c.tab_pair_minus.upload(pm.data(), pm.size(), c.stream);
   c.tab_g_plus.upload(gp.data(), gp.size(), c.stream);
   c.tab_g_minus.upload(gm.data(), gm.size(), c.stream);
   c.tab_pair_plus_ns.upload(ppns.data(), ppns.size(), c.stream);
-  c.tab_pair_back_ns.upload(pbns.data(), pbns.size(), c.stream);
   GB_CUDA(cudaStreamSynchronize(c.stream));
 }
 
@@ -399,8 +392,7 @@ struct GwRun {
     a.B.ptr = c.V.get(); a.B.row = lin(1); a.B.col = lin(nao); a.B.bat.tab0 = tVp;
     a.C.ptr = X1; a.C.row = two(nao, 1, pe); a.C.col = lin(nao);
     a.C.bat.s0 = blkT1;
-    // (b) Bt[t][kk][s][Q][n][r] = sum_p Gbar(nts-1-t, s, k)[r][p] T1[kk][t][s][Q][p][n], stored with
-    //     r (the result row) unit-stride so that the epilogue's stores coalesce
+    // (b) Bt[t][kk][s][Q][r][n] = sum_p Gbar(nts-1-t, s, k)[r][p] T1[kk][t][s][Q][p][n]
     ZGemm b;
     b.M = nao; b.N = (int64_t)NQ * nao; b.K = nao;
     b.nb0 = kbk; b.nb1 = nth; b.nb2 = ns;
@@ -408,18 +400,16 @@ struct GwRun {
     b.A.bat.s0 = ge; b.A.bat.s1 = -g_t; b.A.bat.s2 = g_s;
     b.B.ptr = X1; b.B.row = lin(nao); b.B.col = two(nao, 1, nao2);
     b.B.bat.s0 = blkT1; b.B.bat.s1 = (int64_t)ns * pe; b.B.bat.s2 = pe;
-    b.C.ptr = X2; b.C.row = lin(1); b.C.col = two(nao, nao, nao2);
+    b.C.ptr = X2; b.C.row = lin(nao); b.C.col = two(nao, 1, nao2);
     b.C.bat.s0 = (int64_t)ns * pe; b.C.bat.s1 = (int64_t)kbk * ns * pe; b.C.bat.s2 = pe;
-    // (c) P0[t][Q][Q'] -= pref sum_{(kk,s),(n,r)} Bt[t][(kk,s)][Q][(n,r)] conj(V(k,k+q)[Q'][(r,n)]),
+    // (c) P0[t][Q][Q'] -= pref sum_{(kk,s),(r,n)} Bt[t][(kk,s)][Q][(r,n)] conj(V(k,k+q)[Q'][(r,n)]),
     //     computed as P0^T = conj(V) Bt^T: the tau-independent V is the left operand (sliced
-    //     once per call), Bt the right one; rows Q', columns Q, K = ((kk,s),(n,r)).  With K in
-    //     (n, r) order, conj(V(k,k+q)[Q'][r][n]) is V(k+q,k)[Q'][n][r] (the stored pairs are
-    //     conjugate transposes of each other), read straight from the pair V(k+q, k)
+    //     once per call), Bt the right one; rows Q', columns Q, K = ((kk,s),(r,n))
     ZGemm cc;
     cc.M = NQ; cc.N = NQ; cc.K = (int64_t)kbk * ns * nao2;
     cc.nb0 = 1; cc.nb1 = 1; cc.nb2 = nth;
-    cc.A.ptr = c.V.get(); cc.A.row = lin(nao2);
-    cc.A.col = twotab(nao2, 1, c.tab_pair_back_ns.get() + ((int64_t)q * nk + k0) * ns);
+    cc.A.ptr = c.V.get(); cc.A.row = lin(nao2); cc.A.conj = true;
+    cc.A.col = twotab(nao2, 1, c.tab_pair_plus_ns.get() + ((int64_t)q * nk + k0) * ns);
     cc.B.ptr = X2; cc.B.col = lin(nao2); cc.B.row = two(nao2, 1, (int64_t)NQ * nao2);
     cc.B.bat.s2 = (int64_t)kbk * ns * pe;
     cc.C.ptr = P0; cc.C.row = lin(1); cc.C.col = lin(NQ); cc.C.bat.s2 = (int64_t)NQ * NQ;
